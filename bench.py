@@ -1,0 +1,325 @@
+"""Benchmark of the HistoPyramid marching-cubes hot path on B200.
+
+Workload (one "step" = one extraction of one volume): FP32 512^3 Cayley cubic
+16xyz + 4(x^2+y^2+z^2) - 1 + N(0, 1e-3) on [-1,1]^3, iso 0, central-difference
+normals: classify + reduce (HPMCbuildHistopyramid) and traversal into float4
+position/normal streams (HPMCextractVertices, vertex count read on the device).
+
+  value    Gcells/s with the field resident in HBM (device time, CUDA events)
+  e2e      the same through the public API with host buffers: pinned H2D of
+           the field, build, count (host sync), extraction, D2H of every vertex
+  roofline the build kernels (classify + reduce) against measured HBM copy
+           bandwidth; algorithmic bytes = field bytes read once
+  cpu_baseline  the oracle (CPU restatement of the reference) on a z-slab sample
+
+--impl reference times the reference's path on the host cores instead: the
+reference is GLSL for a GL driver (no GL stack on this box), so its CPU
+restatement (oracle/, OpenMP over all host threads) stands in for it.
+
+N > 1 (torchrun): every rank extracts its own volume (independent objects,
+no collective on the data path): weak scaling, value = all ranks' cells / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcells/s @512³ f32 (% HBM roof); batched vs plain vols/s; adjoint/fwd time"
+WORKLOAD = ("cayley_512: FP32 512^3 lattice, Cayley cubic 16xyz+4(x^2+y^2+z^2)-1 + N(0,1e-3) on [-1,1]^3, "
+            "iso 0, central-difference normals, float4 position+normal streams")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(field_np, iso, threads=0, min_seconds=10.0, slab=64):
+    """The oracle on a z-slab of the workload (bounded sample), repeated >= min_seconds."""
+    from oracle import oracle as O
+
+    sample = np.ascontiguousarray(field_np[: slab + 1])
+    cells = (sample.shape[2] - 1) * (sample.shape[1] - 1) * (sample.shape[0] - 1)
+    t0 = time.perf_counter()
+    runs = 0
+    verts = 0
+    while True:
+        n, _, _ = O.extract_count(sample, iso, normal_mode=O.NORMALS_CENTRAL, threads=threads, geometry=True)
+        verts = n
+        runs += 1
+        if time.perf_counter() - t0 >= min_seconds:
+            break
+    dt = time.perf_counter() - t0
+    cores = threads if threads > 0 else O.max_threads()
+    return {"value": cells * runs / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": "port",
+            "sample": f"z-slab {sample.shape[2]}x{sample.shape[1]}x{sample.shape[0]} of the 512^3 field "
+                      f"({cells} cells, {verts} vertices, codes+pyramid+traversal+FP64 geometry), {runs} runs"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from hpmc_b200 import datasets
+
+    field, iso = datasets.cayley(512)
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    for _ in range(args.warmup):
+        cpu_baseline(field, iso, threads, min_seconds=0.0, slab=16)
+    t0 = time.perf_counter()
+    vals = []
+    for _ in range(args.steps):
+        b = cpu_baseline(field, iso, threads, min_seconds=0.0, slab=32)
+        vals.append(b["value"])
+    dt = time.perf_counter() - t0
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Gcells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "lattice": [512, 512, 512]},
+            "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
+                             "sample": "z-slab 512x512x33 of the 512^3 field per step (oracle, all host threads)"},
+            "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference path is GLSL run by a GL driver: unavailable on this box (no GL stack); "
+                    "its CPU restatement (oracle/) is timed instead"}
+    print(json.dumps(line), flush=True)
+
+
+def run_hpmc(args, rank, world, local_rank):
+    import torch
+
+    import hpmc_b200 as H
+    from hpmc_b200 import datasets
+
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    field_np, iso = datasets.cayley(512)
+    fz, fy, fx = field_np.shape
+    cells = (fx - 1) * (fy - 1) * (fz - 1)
+    field_bytes = field_np.nbytes
+    field = torch.from_numpy(field_np).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    C = H.Constants()
+    hp = H.HistoPyramid(C)
+    hp.set_stream(stream)
+    hp.set_field_device(field)
+    hp.set_normal_mode(H.NORMALS_CENTRAL)
+    hp.build(iso)
+    nverts = hp.acquire_number_of_vertices()
+    th = H.TraversalHandle(hp)
+    pos = torch.empty((nverts, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((nverts, 4), dtype=torch.float32, device=dev)
+    th.set_buffers(pos, nrm, nverts)
+
+    def step():
+        hp.build(iso)
+        th.extract()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    stream.synchronize()
+
+    # --- timed region: field resident in HBM -------------------------------
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        t_begin = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_begin.record(stream)
+        for i in range(args.steps):
+            ev[3 * i].record(stream)
+            hp.build(iso)
+            ev[3 * i + 1].record(stream)
+            th.extract()
+            ev[3 * i + 2].record(stream)
+        t_end.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+    total_ms = t_begin.elapsed_time(t_end)
+    build_ms = [ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps)]
+    trav_ms = [ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps)]
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = cells * world * args.steps / (total_ms * 1e-3) / 1e9
+
+    peak, peak_kind = hbm_peak()
+    build_avg = statistics.mean(build_ms)
+    trav_avg = statistics.mean(trav_ms)
+    out_bytes = 32 * nverts
+    alg_bytes = field_bytes + out_bytes
+    roof = {"kernel": "build = classify_column_tma + reduce_levels (classify dominates)",
+            "bound": "hbm", "achieved": field_bytes / (build_avg * 1e-3) / 1e9, "peak": peak,
+            "unit": "GB/s", "frac": field_bytes / (build_avg * 1e-3) / 1e9 / peak, "traffic": None,
+            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": field_bytes,
+            "avg_launch_ms": build_avg}
+    step_frac = alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak
+
+    # --- e2e through the public API with host buffers ----------------------
+    e2e = None
+    if rank == 0 or world > 1:
+        h_field = torch.from_numpy(field_np).pin_memory()
+        h_pos = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
+        h_nrm = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
+        e2e_steps = max(3, min(args.steps, 10))
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                field.copy_(h_field, non_blocking=True)
+                hp.build(iso)
+                n = hp.acquire_number_of_vertices()
+                th.extract()
+                h_pos[:n].copy_(pos[:n], non_blocking=True)
+                h_nrm[:n].copy_(nrm[:n], non_blocking=True)
+            stream.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(e2e_steps):
+                field.copy_(h_field, non_blocking=True)
+                hp.build(iso)
+                n = hp.acquire_number_of_vertices()
+                th.extract()
+                h_pos[:n].copy_(pos[:n], non_blocking=True)
+                h_nrm[:n].copy_(nrm[:n], non_blocking=True)
+            e1.record(stream)
+            stream.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e2e_steps
+        assert n == nverts
+        e2e = {"value": cells / (e2e_ms * 1e-3) / 1e9, "unit": "Gcells/s", "h2d_bytes_per_step": field_bytes,
+               "d2h_bytes_per_step": 32 * nverts, "ms_per_step": e2e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(field_np, iso)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic: seeded Cayley cubic + N(0,1e-3) noise, generated in FP64, stored FP32",
+                "config": {"workload": WORKLOAD, "lattice": [fx, fy, fz], "cells": cells, "vertices": nverts,
+                           "normals": "central", "l2": "inputs larger than L2 (537 MB field per step)",
+                           "parallelism": f"replicas x{world} (independent volumes)"},
+                "roofline": roof,
+                "step_hbm_fraction": step_frac,
+                "step_algorithmic_bytes": alg_bytes,
+                "vertices_per_s": nverts * world * args.steps / (total_ms * 1e-3),
+                "build_ms": build_avg, "traverse_ms": trav_avg,
+                "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 3 * args.steps,
+                "clocks": clocks.summary()}
+        print(json.dumps(line), flush=True)
+    th.close()
+    hp.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="hpmc", choices=["hpmc", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_hpmc(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,746 @@
+// hpmc_api.cu -- host runtime and C ABI (include/hpmc.h).
+//
+// Mirrors the reference's handle model (hpmc/include/hpmc_internal.h:67-211):
+// constants, a HistoPyramid per volume configuration with lazy set-up on a
+// "tainted" flag and a sticky "broken" flag, and traversal handles.  GL
+// objects become device allocations; the pass driver of buildpass.cpp:42-178
+// becomes two kernel launches (classify, reduce) on the handle's stream and
+// the draw loop of triface.cpp:423-428 becomes one persistent traversal launch.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "hpmc.h"
+#include "hpmc_device.cuh"
+#include "hpmc_kernels.h"
+
+using hpmc::Ctrl;
+using hpmc::Volume;
+
+namespace {
+
+constexpr uint32_t kMagicConstants = 0x48504331u;  // "HPC1"
+constexpr uint32_t kMagicPyramid = 0x48505931u;
+constexpr uint32_t kMagicTraversal = 0x48505431u;
+
+struct FieldDesc {
+    const void* ptr = nullptr;
+    int type = HPMC_SCALAR_F32;
+    int size[3] = {0, 0, 0};
+    size_t row_pitch = 0;    // bytes, 0 = dense
+    size_t slice_pitch = 0;  // bytes, 0 = dense
+};
+
+std::mutex g_fields_mu;
+std::map<GLuint, FieldDesc> g_fields;
+GLuint g_next_field = 1;
+
+// ---------------------------------------------------------------------------
+// init.cpp:72-149 -- layout of the tiled base level.  For a 1-cell axis the
+// reference shifts by -1 (undefined); the exponent is clamped at 0 here.
+bool determine_layout(const int lattice[3], const int cells[3], int out[6]) {
+    for (int i = 0; i < 3; i++) {
+        if (lattice[i] < 2 || lattice[i] > 16384) return false;  // init.cpp:82-90
+        if (lattice[i] <= cells[i]) return false;                // init.cpp:98-103
+        if (cells[i] < 1) return false;
+    }
+    auto tile_exp = [](int c) {
+        int e = (int)ceilf(log2f(static_cast<float>(c) / 2.0f));  // init.cpp:106-111
+        return e < 0 ? 0 : e;
+    };
+    const int tx = 1 << tile_exp(cells[0]);
+    const int ty = 1 << tile_exp(cells[1]);
+    const float aspect = static_cast<float>(tx) / static_cast<float>(ty);
+    const float lxe = std::max(0.0f, ceilf(log2f(sqrtf(static_cast<float>(cells[2]) / aspect))));
+    const int lx = 1 << static_cast<int>(lxe);                     // init.cpp:116-119
+    const int ly = (cells[2] + lx - 1) / lx;                       // init.cpp:120-121
+    const int l2 = static_cast<int>(ceilf(log2f(static_cast<float>(std::max(tx * lx, ty * ly)))));
+    const int size = 1 << l2;                                      // init.cpp:123-128
+    out[0] = tx;
+    out[1] = ty;
+    out[2] = size / tx;                                            // init.cpp:129-130
+    out[3] = size / ty;
+    out[4] = l2;
+    out[5] = size;
+    return true;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+size_t elem_size(int type) { return type == HPMC_SCALAR_F32 ? 4 : 1; }
+
+}  // namespace
+
+struct HPMCConstants {
+    uint32_t magic;
+    int device;
+    int num_sms;
+    int traverse_ctas_per_sm;
+};
+
+struct HPMCHistoPyramid {
+    uint32_t magic = kMagicPyramid;
+    HPMCConstants* constants = nullptr;
+    bool tainted = true;
+    bool broken = true;  // hpiface.cpp:57
+    int status = HPMC_OK;
+    int lattice[3] = {0, 0, 0};
+    int cells[3] = {0, 0, 0};
+    float extent[3] = {1.f, 1.f, 1.f};
+    bool binary = false;
+    // field source
+    enum { kNone, kArray, kFunctor } fmode = kNone;
+    FieldDesc field;
+    hpmc::FunctorParams functor{};
+    bool gradient = false;
+    int normal_mode = HPMC_NORMALS_FORWARD;
+    cudaStream_t stream = nullptr;
+    // layout
+    int layout[6] = {0, 0, 0, 0, 0, 0};
+    // device state
+    Volume V{};
+    uint32_t* d_levels = nullptr;
+    size_t levels_cap = 0;  // entries
+    uint32_t* d_arena = nullptr;
+    size_t arena_cap = 0;   // slots
+    Ctrl* d_ctrl = nullptr;
+    uint8_t* codes_capture = nullptr;
+    CUtensorMap tmap;
+    bool have_tmap = false;
+    bool built = false;
+    float threshold = 0.f;
+    unsigned long long count_cached = 0;
+    bool count_valid = false;
+};
+
+struct HPMCTraversalHandle {
+    uint32_t magic = kMagicTraversal;
+    HPMCHistoPyramid* h = nullptr;
+    float* pos = nullptr;
+    float* nrm = nullptr;
+    size_t cap = 0;
+    float* feedback = nullptr;
+    size_t feedback_cap = 0;
+    int32_t* dbg_cell = nullptr;
+    float* dbg_t = nullptr;
+};
+
+namespace {
+
+bool valid(const HPMCHistoPyramid* h) { return h && h->magic == kMagicPyramid; }
+bool valid(const HPMCTraversalHandle* th) { return th && th->magic == kMagicTraversal && valid(th->h); }
+
+void set_error(HPMCHistoPyramid* h, int status, bool brk) {
+    h->status = status;
+    if (brk) h->broken = true;
+}
+
+void release_device(HPMCHistoPyramid* h) {
+    cudaFree(h->d_levels);
+    cudaFree(h->d_arena);
+    cudaFree(h->d_ctrl);
+    h->d_levels = nullptr;
+    h->d_arena = nullptr;
+    h->d_ctrl = nullptr;
+    h->levels_cap = h->arena_cap = 0;
+}
+
+// Resolve the field source into the Volume's field members.
+int bind_field(HPMCHistoPyramid* h) {
+    Volume& V = h->V;
+    if (h->fmode == HPMCHistoPyramid::kFunctor) {
+        V.ftype = hpmc::kFieldFunctor;
+        V.field = nullptr;
+        V.row_pitch = V.slice_pitch = 0;
+        V.functor = h->functor;
+        return HPMC_OK;
+    }
+    if (h->fmode != HPMCHistoPyramid::kArray || !h->field.ptr) return HPMC_ERR_NO_FIELD;
+    const FieldDesc& f = h->field;
+    const size_t es = elem_size(f.type);
+    const size_t rp = f.row_pitch ? f.row_pitch : (size_t)h->lattice[0] * es;
+    const size_t sp = f.slice_pitch ? f.slice_pitch : rp * (size_t)h->lattice[1];
+    if (rp % es || sp % es || rp < (size_t)h->lattice[0] * es || sp < rp * (size_t)h->lattice[1])
+        return HPMC_ERR_INVALID_VALUE;
+    V.field = f.ptr;
+    V.ftype = f.type == HPMC_SCALAR_F32 ? hpmc::kFieldF32
+              : f.type == HPMC_SCALAR_U8 ? hpmc::kFieldU8
+                                         : hpmc::kFieldUNorm8;
+    V.row_pitch = (long long)(rp / es);
+    V.slice_pitch = (long long)(sp / es);
+    // TMA column path: column layout, 16-byte aligned base and pitches
+    h->have_tmap = false;
+    if (V.column_layout && ((uintptr_t)f.ptr % 16 == 0) && rp % 16 == 0 && sp % 16 == 0) {
+        auto enc = tensor_map_encoder();
+        if (enc) {
+            const cuuint64_t dims[3] = {(cuuint64_t)h->lattice[0], (cuuint64_t)h->lattice[1],
+                                        (cuuint64_t)h->lattice[2]};
+            const cuuint64_t strides[2] = {(cuuint64_t)rp, (cuuint64_t)sp};
+            const bool f32 = f.type == HPMC_SCALAR_F32;
+            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, 1u};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            CUresult r = enc(&h->tmap, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                             const_cast<void*>(f.ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            h->have_tmap = (r == CUDA_SUCCESS);
+        }
+    }
+    return HPMC_OK;
+}
+
+// HPMCsetup (init.cpp:48-69): layout + device memory for it.
+bool setup(HPMCHistoPyramid* h) {
+    if (!h->tainted) return true;
+    int L[6];
+    if (!determine_layout(h->lattice, h->cells, L)) {
+        h->status = HPMC_ERR_LAYOUT;
+        return false;
+    }
+    std::memcpy(h->layout, L, sizeof L);
+    Volume& V = h->V;
+    V = Volume{};
+    for (int i = 0; i < 3; i++) {
+        V.lattice[i] = h->lattice[i];
+        V.cells[i] = h->cells[i];
+        V.scale[i] = h->extent[i] / (float)h->cells[i];
+    }
+    V.tile_x = L[0];
+    V.tile_y = L[1];
+    V.layout_x = L[2];
+    V.layout_y = L[3];
+    V.size_l2 = L[4];
+    V.jtop = std::max(hpmc::kBlockLevel, V.size_l2 + 1);
+    // dense levels, top first, each padded to a multiple of 4 entries
+    long long off = 0;
+    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
+        V.level_off[j] = off;
+        off += (hpmc::level_entries(V.size_l2, j) + 3) & ~3ll;
+    }
+    const long long levels_total = off;
+    V.nblocks = hpmc::level_entries(V.size_l2, hpmc::kBlockLevel);
+    V.top_cached = 0;
+    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
+        const long long end = V.level_off[j] + ((hpmc::level_entries(V.size_l2, j) + 3) & ~3ll);
+        if (end > hpmc::kTopCacheEntries) break;
+        V.top_cached = (int)end;
+    }
+    V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
+    V.nfx = (V.cells[0] + 31) / 32;
+    V.nfy = (V.cells[1] + 31) / 32;
+    const long long slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
+    // (re)allocate
+    if ((size_t)levels_total > h->levels_cap || (size_t)slots > h->arena_cap || !h->d_ctrl) {
+        release_device(h);
+        if (cudaMalloc(&h->d_levels, sizeof(uint32_t) * levels_total) != cudaSuccess ||
+            cudaMalloc(&h->d_arena, sizeof(uint32_t) * hpmc::kBlockWords * (size_t)slots) != cudaSuccess ||
+            cudaMalloc(&h->d_ctrl, sizeof(Ctrl)) != cudaSuccess) {
+            cudaGetLastError();
+            release_device(h);
+            h->status = HPMC_ERR_OUT_OF_MEMORY;
+            return false;
+        }
+        h->levels_cap = (size_t)levels_total;
+        h->arena_cap = (size_t)slots;
+    }
+    if (cudaMemset(h->d_ctrl, 0, sizeof(Ctrl)) != cudaSuccess ||
+        cudaMemset(h->d_levels, 0, sizeof(uint32_t) * levels_total) != cudaSuccess) {
+        h->status = HPMC_ERR_CUDA;
+        return false;
+    }
+    V.levels = h->d_levels;
+    V.arena = h->d_arena;
+    V.arena_slots = slots;
+    V.ctrl = h->d_ctrl;
+    h->tainted = false;
+    h->built = false;
+    h->count_valid = false;
+    return true;
+}
+
+int traverse_grid(const HPMCHistoPyramid* h) {
+    const HPMCConstants* c = h->constants;
+    int grid = c->num_sms * c->traverse_ctas_per_sm;
+    if (h->count_valid) {
+        const unsigned long long per_cta = 32ull * hpmc::kTraverseRounds * hpmc::kWarps;
+        const unsigned long long need = (h->count_cached + per_cta - 1) / per_cta;
+        grid = (int)std::max<unsigned long long>(1, std::min<unsigned long long>((unsigned long long)grid, need));
+    }
+    return grid;
+}
+
+int launch_extract(HPMCTraversalHandle* th, float* pos, float* nrm, float* feedback, size_t cap) {
+    HPMCHistoPyramid* h = th->h;
+    if (h->broken) return HPMC_ERR_BROKEN;
+    if (!h->built) return HPMC_ERR_NOT_BUILT;
+    hpmc::TraverseOut O{};
+    O.pos = reinterpret_cast<float4*>(pos);
+    O.nrm = reinterpret_cast<float4*>(nrm);
+    O.feedback = feedback;
+    O.capacity = cap;
+    O.dbg_cell = reinterpret_cast<int4*>(th->dbg_cell);
+    O.dbg_t = th->dbg_t;
+    if (h->count_valid && h->count_cached > cap) h->status = HPMC_ERR_CAPACITY;
+    cudaError_t e = hpmc::launch_traverse(h->V, O, h->normal_mode, traverse_grid(h), h->stream);
+    if (e != cudaSuccess) {
+        set_error(h, HPMC_ERR_CUDA, true);
+        return HPMC_ERR_CUDA;
+    }
+    return (h->count_valid && h->count_cached > cap) ? HPMC_ERR_CAPACITY : HPMC_OK;
+}
+
+}  // namespace
+
+// ============================== C ABI ======================================
+extern "C" {
+
+HPMCConstants* HPMCcreateConstants(GLint max_gl_major, GLint max_gl_minor) {
+    (void)max_gl_minor;
+    if (max_gl_major < 2) return nullptr;  // constants.cpp:115-123
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    auto* c = new (std::nothrow) HPMCConstants;
+    if (!c) return nullptr;
+    c->magic = kMagicConstants;
+    c->device = dev;
+    c->num_sms = prop.multiProcessorCount;
+    c->traverse_ctas_per_sm = hpmc::traverse_blocks_per_sm();
+    hpmc::column_smem_ok();
+    return c;
+}
+
+void HPMCdestroyConstants(HPMCConstants* c) {
+    if (!c || c->magic != kMagicConstants) return;
+    c->magic = 0;
+    delete c;
+}
+
+HPMCHistoPyramid* HPMCcreateHistoPyramid(HPMCConstants* s) {
+    if (!s || s->magic != kMagicConstants) return nullptr;
+    auto* h = new (std::nothrow) HPMCHistoPyramid;
+    if (!h) return nullptr;
+    h->constants = s;
+    return h;
+}
+
+void HPMCsetLatticeSize(HPMCHistoPyramid* h, GLsizei x, GLsizei y, GLsizei z) {
+    if (!valid(h)) return;
+    h->lattice[0] = x;
+    h->lattice[1] = y;
+    h->lattice[2] = z;
+    h->cells[0] = std::max(1, x) - 1;
+    h->cells[1] = std::max(1, y) - 1;
+    h->cells[2] = std::max(1, z) - 1;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+}
+
+void HPMCsetFieldAsBinary(HPMCHistoPyramid* h) {
+    if (valid(h)) h->binary = true;
+}
+
+void HPMCsetFieldAsContinuous(HPMCHistoPyramid* h) {
+    if (valid(h)) h->binary = false;
+}
+
+void HPMCsetGridSize(HPMCHistoPyramid* h, GLsizei x, GLsizei y, GLsizei z) {
+    if (!valid(h)) return;
+    h->cells[0] = x;
+    h->cells[1] = y;
+    h->cells[2] = z;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+}
+
+void HPMCsetGridExtent(HPMCHistoPyramid* h, GLfloat x, GLfloat y, GLfloat z) {
+    if (!valid(h)) return;
+    h->extent[0] = x;
+    h->extent[1] = y;
+    h->extent[2] = z;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+}
+
+void HPMCsetFieldTexture3D(HPMCHistoPyramid* h, GLuint texture, GLboolean gradient) {
+    if (!valid(h)) return;
+    if (gradient) {
+        set_error(h, HPMC_ERR_UNSUPPORTED, true);
+        return;
+    }
+    FieldDesc f;
+    {
+        std::lock_guard<std::mutex> lk(g_fields_mu);
+        auto it = g_fields.find(texture);
+        if (it == g_fields.end()) {
+            set_error(h, HPMC_ERR_INVALID_VALUE, true);
+            return;
+        }
+        f = it->second;
+    }
+    h->fmode = HPMCHistoPyramid::kArray;
+    h->field = f;
+    h->gradient = false;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+}
+
+void HPMCsetFieldCustom(HPMCHistoPyramid* h, const char* src, GLuint builder_texunit, GLboolean gradient) {
+    (void)builder_texunit;
+    if (!valid(h)) return;
+    int id = 0;
+    if (src) {
+        const std::string s(src);
+        if (s == "hpmc:cayley") id = 1;
+        else if (s == "hpmc:metaballs") id = 2;
+        else if (s == "hpmc:twist_metaballs") id = 3;
+        else if (s == "hpmc:spheres") id = 4;
+    }
+    if (!id) {
+        set_error(h, HPMC_ERR_UNSUPPORTED, true);
+        return;
+    }
+    h->fmode = HPMCHistoPyramid::kFunctor;
+    h->functor = hpmc::FunctorParams{};
+    h->functor.id = id;
+    h->gradient = gradient != 0;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+}
+
+GLuint HPMCgetBuilderProgram(HPMCHistoPyramid* h) {
+    if (!valid(h) || h->broken) return 0;
+    if (h->tainted && !setup(h)) return 0;
+    return h->fmode == HPMCHistoPyramid::kFunctor ? 0x100u + (GLuint)h->functor.id : 0u;
+}
+
+void HPMCdestroyHandle(HPMCHistoPyramid* h) {
+    if (!valid(h)) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    release_device(h);
+    h->magic = 0;
+    delete h;
+}
+
+void HPMCbuildHistopyramid(HPMCHistoPyramid* h, GLfloat threshold) {
+    if (!valid(h) || h->broken) return;  // hpiface.cpp:229-231
+    if (h->tainted && !setup(h)) return;  // hpiface.cpp:253-260: stays tainted, nothing built
+    int st = bind_field(h);
+    if (st != HPMC_OK) {
+        set_error(h, st, true);
+        return;
+    }
+    Volume& V = h->V;
+    V.iso = threshold;
+    V.binary = h->binary ? 1 : 0;
+    V.codes_out = h->codes_capture;
+    h->threshold = threshold;
+    const int max_ctas = h->constants->num_sms * 16;
+    cudaError_t e = hpmc::launch_classify(V, h->have_tmap ? &h->tmap : nullptr, max_ctas, h->stream);
+    if (e == cudaSuccess) e = hpmc::launch_reduce(V, h->stream);
+    if (e != cudaSuccess) {
+        set_error(h, HPMC_ERR_CUDA, true);  // hpiface.cpp:263-266
+        return;
+    }
+    h->built = true;
+    h->count_valid = false;
+}
+
+GLuint HPMCacquireNumberOfVertices(HPMCHistoPyramid* h) {
+    if (!valid(h) || h->broken) return 0;  // hpiface.cpp:296-298
+    if (!h->built) return 0;               // init.cpp:146-147: count starts at zero
+    if (!h->count_valid) {
+        Ctrl c;
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+            cudaMemcpy(&c, h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            set_error(h, HPMC_ERR_CUDA, true);
+            return 0;
+        }
+        if (c.status & hpmc::kStatusTimeout) {
+            set_error(h, HPMC_ERR_TIMEOUT, true);
+            return 0;
+        }
+        if ((c.status & hpmc::kStatusOverflow) || c.total > 0xffffffffull) {
+            h->status = HPMC_ERR_OVERFLOW;
+            return 0;
+        }
+        h->count_cached = c.total;
+        h->count_valid = true;
+    }
+    return (GLuint)h->count_cached;
+}
+
+HPMCTraversalHandle* HPMCcreateTraversalHandle(HPMCHistoPyramid* h) {
+    if (!valid(h)) return nullptr;
+    if (!setup(h)) return nullptr;  // triface.cpp:79-84
+    auto* th = new (std::nothrow) HPMCTraversalHandle;
+    if (!th) return nullptr;
+    th->h = h;
+    return th;
+}
+
+void HPMCdestroyTraversalHandle(HPMCTraversalHandle* th) {
+    if (!th || th->magic != kMagicTraversal) return;
+    th->magic = 0;
+    delete th;
+}
+
+char* HPMCgetTraversalShaderFunctions(HPMCTraversalHandle* th) {
+    if (valid(th)) th->h->status = HPMC_ERR_UNSUPPORTED;
+    return nullptr;
+}
+
+bool HPMCsetTraversalHandleProgram(HPMCTraversalHandle* th, GLuint, GLuint, GLuint, GLuint) {
+    if (valid(th)) th->h->status = HPMC_ERR_UNSUPPORTED;
+    return false;
+}
+
+bool HPMCextractVertices(HPMCTraversalHandle* th) {
+    if (!valid(th)) return false;
+    if (!th->pos && !th->nrm) return false;  // triface.cpp:350-355: no program bound
+    const int st = launch_extract(th, th->pos, th->nrm, nullptr, th->cap);
+    if (st != HPMC_OK) th->h->status = st;
+    return st == HPMC_OK;
+}
+
+static bool extract_feedback(HPMCTraversalHandle* th) {
+    if (!valid(th) || !th->feedback) return false;
+    const int st = launch_extract(th, nullptr, nullptr, th->feedback, th->feedback_cap);
+    if (st != HPMC_OK) th->h->status = st;
+    return st == HPMC_OK;
+}
+
+bool HPMCextractVerticesTransformFeedback(HPMCTraversalHandle* th) { return extract_feedback(th); }
+bool HPMCextractVerticesTransformFeedbackNV(HPMCTraversalHandle* th) { return extract_feedback(th); }
+bool HPMCextractVerticesTransformFeedbackEXT(HPMCTraversalHandle* th) { return extract_feedback(th); }
+
+// ------------------------------------------------------------------------
+int HPMCgetLastError(HPMCHistoPyramid* h) { return valid(h) ? h->status : HPMC_ERR_INVALID_HANDLE; }
+
+GLuint HPMCregisterDeviceField(const void* ptr, int type, GLsizei x, GLsizei y, GLsizei z, size_t row_pitch,
+                               size_t slice_pitch) {
+    if (!ptr || x < 1 || y < 1 || z < 1 || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_UNORM8) return 0;
+    FieldDesc f;
+    f.ptr = ptr;
+    f.type = type;
+    f.size[0] = x;
+    f.size[1] = y;
+    f.size[2] = z;
+    f.row_pitch = row_pitch;
+    f.slice_pitch = slice_pitch;
+    std::lock_guard<std::mutex> lk(g_fields_mu);
+    const GLuint name = g_next_field++;
+    g_fields[name] = f;
+    return name;
+}
+
+void HPMCunregisterDeviceField(GLuint name) {
+    std::lock_guard<std::mutex> lk(g_fields_mu);
+    g_fields.erase(name);
+}
+
+int HPMCsetFieldDevice(HPMCHistoPyramid* h, const void* ptr, int type, size_t row_pitch, size_t slice_pitch) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!ptr || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_UNORM8) {
+        h->status = HPMC_ERR_INVALID_VALUE;
+        return h->status;
+    }
+    h->fmode = HPMCHistoPyramid::kArray;
+    h->field = FieldDesc{};
+    h->field.ptr = ptr;
+    h->field.type = type;
+    h->field.row_pitch = row_pitch;
+    h->field.slice_pitch = slice_pitch;
+    h->gradient = false;
+    h->tainted = true;
+    h->broken = false;
+    h->status = HPMC_OK;
+    return HPMC_OK;
+}
+
+int HPMCsetBuilderUniforms(HPMCHistoPyramid* h, const float* values, int count) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (h->fmode != HPMCHistoPyramid::kFunctor || count < 0 || count > hpmc::kFunctorMaxParams ||
+        (count && !values)) {
+        h->status = HPMC_ERR_INVALID_VALUE;
+        return h->status;
+    }
+    h->functor.count = count;
+    for (int i = 0; i < count; i++) h->functor.p[i] = values[i];
+    h->V.functor = h->functor;
+    return HPMC_OK;
+}
+
+int HPMCsetStream(HPMCHistoPyramid* h, void* stream) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    h->stream = static_cast<cudaStream_t>(stream);
+    return HPMC_OK;
+}
+
+int HPMCsetNormalMode(HPMCHistoPyramid* h, int mode) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (mode != HPMC_NORMALS_FORWARD && mode != HPMC_NORMALS_CENTRAL) return HPMC_ERR_INVALID_VALUE;
+    h->normal_mode = mode;
+    return HPMC_OK;
+}
+
+int HPMCgetDeviceVertexCount(HPMCHistoPyramid* h, const unsigned long long** device_count) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!device_count) return HPMC_ERR_INVALID_VALUE;
+    if (h->tainted && !setup(h)) return h->status;
+    *device_count = &h->d_ctrl->total;
+    return HPMC_OK;
+}
+
+int HPMCsetTraversalHandleBuffers(HPMCTraversalHandle* th, float* pos, float* nrm, size_t cap) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    if ((pos && (uintptr_t)pos % 16) || (nrm && (uintptr_t)nrm % 16)) return HPMC_ERR_INVALID_VALUE;
+    th->pos = pos;
+    th->nrm = nrm;
+    th->cap = cap;
+    return HPMC_OK;
+}
+
+int HPMCsetTraversalHandleFeedbackBuffer(HPMCTraversalHandle* th, float* buf, size_t cap) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    if (buf && (uintptr_t)buf % 8) return HPMC_ERR_INVALID_VALUE;
+    th->feedback = buf;
+    th->feedback_cap = cap;
+    return HPMC_OK;
+}
+
+int HPMCextractVerticesToBuffers(HPMCTraversalHandle* th, float* pos, float* nrm, size_t cap, uint64_t* n_written) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    if ((pos && (uintptr_t)pos % 16) || (nrm && (uintptr_t)nrm % 16)) return HPMC_ERR_INVALID_VALUE;
+    int st = launch_extract(th, pos, nrm, nullptr, cap);
+    if (st != HPMC_OK && st != HPMC_ERR_CAPACITY) return st;
+    if (n_written) {
+        Ctrl c;
+        if (cudaStreamSynchronize(th->h->stream) != cudaSuccess ||
+            cudaMemcpy(&c, th->h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            set_error(th->h, HPMC_ERR_CUDA, true);
+            return HPMC_ERR_CUDA;
+        }
+        *n_written = c.written;
+        if (c.total > cap) st = HPMC_ERR_CAPACITY;
+    }
+    return st;
+}
+
+int HPMCextractVerticesAdjoint(HPMCTraversalHandle* th, const float* dpos, const float* dnrm, uint64_t count,
+                               float* dfield) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    HPMCHistoPyramid* h = th->h;
+    if (h->broken) return HPMC_ERR_BROKEN;
+    if (!h->built) return HPMC_ERR_NOT_BUILT;
+    if (!dfield || (dpos && (uintptr_t)dpos % 16) || (dnrm && (uintptr_t)dnrm % 16)) return HPMC_ERR_INVALID_VALUE;
+    if (h->V.ftype == hpmc::kFieldFunctor) return HPMC_ERR_UNSUPPORTED;
+    if (h->binary) return HPMC_OK;  // midpoints and table normals: no dependence on f
+    hpmc::AdjointIO A{};
+    A.dpos = reinterpret_cast<const float4*>(dpos);
+    A.dnrm = reinterpret_cast<const float4*>(dnrm);
+    A.dfield = dfield;
+    A.count = count;
+    cudaError_t e = hpmc::launch_adjoint(h->V, A, h->normal_mode, traverse_grid(h), h->stream);
+    if (e != cudaSuccess) {
+        set_error(h, HPMC_ERR_CUDA, true);
+        return HPMC_ERR_CUDA;
+    }
+    return HPMC_OK;
+}
+
+int HPMCsetCodeCapture(HPMCHistoPyramid* h, uint8_t* device_codes) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    h->codes_capture = device_codes;
+    return HPMC_OK;
+}
+
+int HPMCgetLayout(HPMCHistoPyramid* h, int out[6]) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!out) return HPMC_ERR_INVALID_VALUE;
+    if (h->tainted && !setup(h)) return h->status;
+    std::memcpy(out, h->layout, sizeof h->layout);
+    return HPMC_OK;
+}
+
+int HPMCreadLevel(HPMCHistoPyramid* h, int level, uint32_t* host_out, size_t entries) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!h->built) return HPMC_ERR_NOT_BUILT;
+    const Volume& V = h->V;
+    if (level < hpmc::kBlockLevel || level > V.jtop || !host_out) return HPMC_ERR_INVALID_VALUE;
+    const long long n = hpmc::level_entries(V.size_l2, level);
+    if ((size_t)n > entries) return HPMC_ERR_INVALID_VALUE;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(host_out, V.levels + V.level_off[level], sizeof(uint32_t) * n, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+        return HPMC_ERR_CUDA;
+    if (level == hpmc::kBlockLevel && V.column_layout) {
+        // entries of padding blocks are never written by the column kernel
+        for (long long b = 0; b < n; b++) {
+            int z, fx, fy;
+            if (!hpmc::column_block(V, (uint64_t)b, z, fx, fy)) host_out[b] = 0;
+        }
+    }
+    return HPMC_OK;
+}
+
+int HPMCsetTraversalDebugBuffers(HPMCTraversalHandle* th, int32_t* cell_info, float* t) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    if (cell_info && (uintptr_t)cell_info % 16) return HPMC_ERR_INVALID_VALUE;
+    th->dbg_cell = cell_info;
+    th->dbg_t = t;
+    return HPMC_OK;
+}
+
+int HPMCgetDeviceStatus(HPMCHistoPyramid* h, unsigned int* status) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!status) return HPMC_ERR_INVALID_VALUE;
+    if (!h->d_ctrl) {
+        *status = 0;
+        return HPMC_OK;
+    }
+    Ctrl c;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(&c, h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return HPMC_ERR_CUDA;
+    *status = c.status;
+    const unsigned int zero = 0;
+    cudaMemcpy(&h->d_ctrl->status, &zero, sizeof zero, cudaMemcpyHostToDevice);
+    return HPMC_OK;
+}
+
+}  // extern "C"

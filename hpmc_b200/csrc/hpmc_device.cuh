@@ -1,0 +1,180 @@
+// hpmc_device.cuh -- device-side data model of the B200 HistoPyramid extractor.
+//
+// The reference keeps its pyramid as one square RGBA32F mip chain whose base
+// level tiles the z-slices in 2-D (hpmc/src/init.cpp:105-130,
+// hpmc/src/texfbosetup.cpp:72-92).  Every cell (x,y,z) gets a virtual 2-D
+// cell coordinate X = 2*tile_x*(z mod layout_x) + x, Y = 2*tile_y*(z div layout_x) + y
+// (shadergen.cpp:103-104, 497-503) and the pyramid's child order
+// r,g,b,a = (0,0),(1,0),(0,1),(1,1) (shadergen.cpp:148-153, 215-218) makes the
+// vertex order the Morton order of (X, Y), X on the even bits.
+//
+// Here the same key space is stored compactly:
+//   * a "block" is an aligned Morton range of 4^5 = 1024 keys (a 32x32 square
+//     of virtual cells);
+//   * dense level j (j >= 5) holds, per aligned range of 4^j keys, its vertex
+//     count as uint32 -- level j equals the reference's mip level j flattened
+//     channel by channel (level j texel t, channel c <-> entry 4*morton(t)+c);
+//   * below block level nothing is stored densely: each block with a non-zero
+//     count gets a 1 KiB "arena" slot holding its 1024 MC codes in Morton
+//     order (4 codes per uint32 word), from which the traversal recomputes
+//     the per-cell counts.  Levels 0..4 of the reference are thus implied by
+//     the codes; codes of empty blocks are all 0 or 255 and are not needed.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hpmc_config.h"
+
+namespace hpmc {
+
+constexpr int kBlockLevel = 5;       // 4^5 keys per block
+constexpr int kBlockKeys = 1024;
+constexpr int kBlockWords = 256;     // arena words per block (4 codes / word)
+constexpr int kMaxLevels = 40;
+
+enum FieldType : int {
+    kFieldF32 = 0,      // float
+    kFieldU8 = 1,       // uint8 read as float(b)
+    kFieldUNorm8 = 2,   // uint8 read as b/255 (GL_ALPHA UNSIGNED_BYTE texture)
+    kFieldFunctor = 3,  // registered device functor evaluated at texel centres
+};
+
+enum NormalMode : int {
+    kNormalsForward = 0,  // reference default: iso - lerp(f(a+e), f(b+e), t)
+    kNormalsCentral = 1,  // -lerp(central difference at a, at b, t)
+};
+
+// Device control block of one pyramid (one volume).
+struct Ctrl {
+    unsigned long long total;    // vertex count (top of the pyramid)
+    unsigned int arena_used;     // arena slots handed out by the current build
+    unsigned int reduce_done;    // last-block-done counter of the reduce kernel
+    unsigned int status;         // sticky error bits (kStatus*)
+    unsigned int written;        // vertices written by the last extraction
+    unsigned int active_blocks;  // non-empty blocks of the last build
+    unsigned int pad;
+};
+
+enum : unsigned int {
+    kStatusOverflow = 1u,      // vertex count does not fit the level type
+    kStatusCapacity = 2u,      // output buffer smaller than the vertex count
+    kStatusArena = 4u,         // arena overflow (never expected: sized for all blocks)
+    kStatusTimeout = 8u,       // a bounded wait gave up
+};
+
+// Parameters of a registered field functor (custom fetch).
+struct FunctorParams {
+    int id;          // functor id (hpmc_functors.cuh)
+    int count;       // number of meaningful floats in p
+    float p[kFunctorMaxParams];
+};
+
+// Everything a kernel needs to know about one volume.
+struct Volume {
+    // field
+    const void* field;
+    long long row_pitch;     // elements
+    long long slice_pitch;   // elements
+    int ftype;
+    int lattice[3];
+    int cells[3];
+    float iso;
+    int binary;
+    float scale[3];          // extent / cells
+    // layout (init.cpp:72-149)
+    int tile_x, tile_y;      // texels per tile (cells per tile = 2x)
+    int layout_x, layout_y;
+    int size_l2;
+    // compact pyramid
+    int jtop;                          // top dense level: max(5, size_l2 + 1)
+    uint32_t* levels;                  // dense levels, top level first
+    long long level_off[kMaxLevels];   // entry offset of dense level j (index j), multiple of 4
+    long long nblocks;                 // entries of level 5
+    int top_cached;                    // leading entries of `levels` the traversal caches in smem
+    // Arena slot of a block.  Column layout (every 32x32 block lies inside
+    // one slice tile): slot = (z * nfy + fy) * nfx + fx over the real
+    // footprints, so only real blocks take memory.  Otherwise slot = block.
+    int column_layout;
+    int nfx, nfy;                      // 32-cell footprints per slice in x, y
+    uint32_t* arena;                   // kBlockWords words per slot
+    long long arena_slots;             // capacity of the arena
+    Ctrl* ctrl;
+    // optional capture of every cell's code, [cz][cy][cx] (inspection)
+    uint8_t* codes_out;
+    // custom field
+    FunctorParams functor;
+    unsigned long long vertex_base;    // first output index of this volume (batched)
+};
+
+// --- Morton helpers (X on even bits) ---------------------------------------
+__host__ __device__ __forceinline__ uint32_t morton_compact(uint64_t v) {
+    v &= 0x5555555555555555ull;
+    v = (v | (v >> 1)) & 0x3333333333333333ull;
+    v = (v | (v >> 2)) & 0x0f0f0f0f0f0f0f0full;
+    v = (v | (v >> 4)) & 0x00ff00ff00ff00ffull;
+    v = (v | (v >> 8)) & 0x0000ffff0000ffffull;
+    v = (v | (v >> 16)) & 0x00000000ffffffffull;
+    return (uint32_t)v;
+}
+__host__ __device__ __forceinline__ uint64_t morton_spread(uint64_t v) {
+    v &= 0xffffffffull;
+    v = (v | (v << 16)) & 0x0000ffff0000ffffull;
+    v = (v | (v << 8)) & 0x00ff00ff00ff00ffull;
+    v = (v | (v << 4)) & 0x0f0f0f0f0f0f0f0full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    v = (v | (v << 1)) & 0x5555555555555555ull;
+    return v;
+}
+// 10-bit Morton index inside a block -> (cx, cy) in 0..31
+__host__ __device__ __forceinline__ void morton10(uint32_t m, int& cx, int& cy) {
+    uint32_t x = m & 0x155u, y = (m >> 1) & 0x155u;
+    x = (x | (x >> 1)) & 0x133u; x = (x | (x >> 2)) & 0x10fu; x = (x | (x >> 4)) & 0x1fu;
+    y = (y | (y >> 1)) & 0x133u; y = (y | (y >> 2)) & 0x10fu; y = (y | (y >> 4)) & 0x1fu;
+    cx = (int)x;
+    cy = (int)y;
+}
+
+// Virtual cell (X, Y) -> lattice cell; false for padding (shadergen.cpp:497-503).
+__host__ __device__ __forceinline__ bool virtual_to_cell(const Volume& V, uint32_t X, uint32_t Y,
+                                                         int& x, int& y, int& z) {
+    const uint32_t wx = 2u * (uint32_t)V.tile_x, wy = 2u * (uint32_t)V.tile_y;
+    const uint32_t tu = X / wx, tv = Y / wy;
+    x = (int)(X - tu * wx);
+    y = (int)(Y - tv * wy);
+    if (tu >= (uint32_t)V.layout_x || tv >= (uint32_t)V.layout_y) return false;
+    z = (int)(tv * (uint32_t)V.layout_x + tu);
+    return x < V.cells[0] && y < V.cells[1] && z < V.cells[2];
+}
+
+__host__ __device__ __forceinline__ long long level_entries(int size_l2, int j) {
+    int e = size_l2 + 1 - j;
+    return e <= 0 ? 1ll : (1ll << (2 * e));
+}
+
+// Column layout: block b -> (slice z, footprint fx, fy); false for padding.
+__host__ __device__ __forceinline__ bool column_block(const Volume& V, uint64_t b, int& z, int& fx,
+                                                      int& fy) {
+    const uint32_t X0 = morton_compact(b) << 5, Y0 = morton_compact(b >> 1) << 5;
+    int x0, y0;
+    const bool ok = virtual_to_cell(V, X0, Y0, x0, y0, z);
+    fx = x0 >> 5;
+    fy = y0 >> 5;
+    return ok;
+}
+
+__host__ __device__ __forceinline__ long long block_slot(const Volume& V, uint64_t b) {
+    if (!V.column_layout) return (long long)b;
+    int z, fx, fy;
+    column_block(V, b, z, fx, fy);
+    return ((long long)z * V.nfy + fy) * V.nfx + fx;
+}
+
+// Block index of footprint (fx, fy) of slice z (column layout).
+__host__ __device__ __forceinline__ uint64_t column_block_index(const Volume& V, int z, int fx, int fy) {
+    const uint32_t tu = (uint32_t)z % (uint32_t)V.layout_x, tv = (uint32_t)z / (uint32_t)V.layout_x;
+    const uint32_t X0 = 2u * (uint32_t)V.tile_x * tu + 32u * (uint32_t)fx;
+    const uint32_t Y0 = 2u * (uint32_t)V.tile_y * tv + 32u * (uint32_t)fy;
+    return morton_spread(X0 >> 5) | (morton_spread(Y0 >> 5) << 1);
+}
+
+}  // namespace hpmc

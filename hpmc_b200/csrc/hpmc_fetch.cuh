@@ -1,0 +1,114 @@
+// hpmc_fetch.cuh -- scalar-field access: device arrays and registered functors.
+//
+// Array fields follow the reference's Texture3D fetch (shadergen.cpp:245-268
+// with apps/texture3d/texture3d.cpp:135-139): NEAREST sampling at texel
+// centres with GL_CLAMP, i.e. clamp-to-edge integer indexing.  uint8 arrays
+// read either as float(b) (kFieldU8) or as GL's normalised b/255
+// (kFieldUNorm8, a GL_ALPHA/GL_UNSIGNED_BYTE texture).
+//
+// Functor fields replace the reference's custom GLSL fetch snippet
+// (HPMCsetFieldCustom, hpiface.cpp:187-200; shadergen.cpp:270-286): the
+// snippet's HPMC_fetch(p) receives normalised texel centres
+// p = ((x+0.5)/FX, (y+0.5)/FY, (z+0.5)/FZ) without clamping (hpmc.h:409-444);
+// here a registered device functor receives the same p.
+#pragma once
+#include "hpmc_device.cuh"
+
+namespace hpmc {
+
+enum FunctorId : int {
+    kFunctorCayley = 1,         // apps/cayley/cayley.cpp:75-94 (with gradient)
+    kFunctorMetaballs = 2,      // sum_i r_i^2 / |p - c_i|^2; p = {n, (cx,cy,cz,r) x n}
+    kFunctorTwistMetaballs = 3, // apps/metaballs/metaballs.cpp:72-94; p = {twist, (cx,cy,cz) x 8}
+    kFunctorSpheres = 4,        // signed distance of a union of spheres; p = {n, (cx,cy,cz,r) x n}
+};
+
+__device__ __forceinline__ float functor_value(const FunctorParams& F, float px, float py, float pz) {
+    switch (F.id) {
+        case kFunctorCayley: {
+            float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+            return 1.0f - 16.0f * x * y * z - 4.0f * x * x - 4.0f * y * y - 4.0f * z * z;
+        }
+        case kFunctorMetaballs: {
+            int n = (int)F.p[0];
+            float s = 0.0f;
+            for (int i = 0; i < n; i++) {
+                float dx = px - F.p[1 + 4 * i], dy = py - F.p[2 + 4 * i], dz = pz - F.p[3 + 4 * i];
+                float r = F.p[4 + 4 * i];
+                s += (r * r) / (dx * dx + dy * dy + dz * dz);
+            }
+            return s;
+        }
+        case kFunctorTwistMetaballs: {
+            float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+            float twist = F.p[0];
+            float rot1 = twist * z, rot2 = 0.7f * twist * y;
+            float c1 = cosf(rot1), s1 = sinf(rot1), c2 = cosf(rot2), s2 = sinf(rot2);
+            // GLSL mat3 constructors are column-major: p' = M p
+            float x1 = c1 * x + s1 * y, y1 = -s1 * x + c1 * y, z1 = z;
+            float x2 = c2 * x1 + s2 * z1, y2 = y1, z2 = -s2 * x1 + c2 * z1;
+            x = 0.5f * x2 + 0.5f;
+            y = 0.5f * y2 + 0.5f;
+            z = 0.5f * z2 + 0.5f;
+            float s = 0.0f;
+            for (int i = 0; i < 8; i++) {
+                float dx = x - F.p[1 + 3 * i], dy = y - F.p[2 + 3 * i], dz = z - F.p[3 + 3 * i];
+                s += 0.05f / (dx * dx + dy * dy + dz * dz);
+            }
+            return s;
+        }
+        case kFunctorSpheres: {
+            int n = (int)F.p[0];
+            float d = 3.0e38f;
+            for (int i = 0; i < n; i++) {
+                float dx = px - F.p[1 + 4 * i], dy = py - F.p[2 + 4 * i], dz = pz - F.p[3 + 4 * i];
+                d = fminf(d, sqrtf(dx * dx + dy * dy + dz * dz) - F.p[4 + 4 * i]);
+            }
+            return d;
+        }
+        default:
+            return 0.0f;
+    }
+}
+
+// Analytic gradient where the functor provides one (HPMC_fetchGrad).
+__device__ __forceinline__ void functor_gradient(const FunctorParams& F, float px, float py, float pz,
+                                                 float& gx, float& gy, float& gz) {
+    if (F.id == kFunctorCayley) {
+        float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        gx = -16.0f * y * z - 8.0f * x;
+        gy = -16.0f * x * z - 8.0f * y;
+        gz = -16.0f * x * y - 8.0f * z;
+    } else {
+        gx = gy = gz = 0.0f;
+    }
+}
+
+template <int FT>
+__device__ __forceinline__ float fetch_raw(const Volume& V, long long off) {
+    if constexpr (FT == kFieldF32) {
+        return __ldg(static_cast<const float*>(V.field) + off);
+    } else if constexpr (FT == kFieldU8) {
+        return (float)__ldg(static_cast<const unsigned char*>(V.field) + off);
+    } else {
+        return __fdiv_rn((float)__ldg(static_cast<const unsigned char*>(V.field) + off), 255.0f);
+    }
+}
+
+// f(x,y,z) with the reference's addressing; x,y,z may lie outside the lattice.
+template <int FT>
+__device__ __forceinline__ float fetch(const Volume& V, int x, int y, int z) {
+    if constexpr (FT == kFieldFunctor) {
+        float px = ((float)x + 0.5f) / (float)V.lattice[0];
+        float py = ((float)y + 0.5f) / (float)V.lattice[1];
+        float pz = ((float)z + 0.5f) / (float)V.lattice[2];
+        return functor_value(V.functor, px, py, pz);
+    } else {
+        x = min(max(x, 0), V.lattice[0] - 1);
+        y = min(max(y, 0), V.lattice[1] - 1);
+        z = min(max(z, 0), V.lattice[2] - 1);
+        return fetch_raw<FT>(V, (long long)z * V.slice_pitch + (long long)y * V.row_pitch + x);
+    }
+}
+
+}  // namespace hpmc

@@ -1,0 +1,416 @@
+// kernels_traverse.cu -- per-vertex HistoPyramid traversal, geometry and the
+// adjoint, on sm_100a.
+//
+// Reference: the traversal vertex shader extractVertex (shadergen.cpp:436-565,
+// GL3+ path) driven by HPMCextractVertices (triface.cpp:332-457), one
+// invocation per output vertex in batches of 3000 (constants.cpp:198).
+//
+// Here one persistent grid walks the vertex range; a warp owns 32 consecutive
+// vertices per round:
+//   1. descent: each lane descends the dense levels from the top (cached in
+//      shared memory) to its 1024-key block, choosing the first child whose
+//      running sum exceeds the key exactly as shadergen.cpp:448-467 does; lanes
+//      of a warp read the same entries, so the loads broadcast.  A warp keeps
+//      its current block and skips the descent for vertices inside it.
+//   2. in-block lookup (warp-cooperative): the warp loads the block's 1024
+//      codes from the arena, each lane turns 32 of them into vertex counts,
+//      a warp scan gives the block's per-cell prefix sums in shared memory,
+//      and each lane binary-searches its key (shadergen.cpp:469-495).
+//   3. geometry (shadergen.cpp:497-563): edge from the case table, crossing
+//      parameter t, position and normal in FP32; coalesced float4 stores.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "hpmc_device.cuh"
+#include "hpmc_fetch.cuh"
+#include "hpmc_kernels.h"
+#include "_gen/hpmc_case_tables.h"
+
+namespace hpmc {
+
+__constant__ uint8_t c_vertex_count_t[256] = HPMC_GEN_VERTEX_COUNT;
+__constant__ uint64_t c_edge_nibbles[256] = HPMC_GEN_EDGE_NIBBLES;
+__device__ const float g_binary_normals[256 * 16 * 3] = HPMC_GEN_BINARY_NORMALS;
+constexpr uint64_t kEdgeGeometry = HPMC_GEN_EDGE_GEOMETRY;
+
+enum { kModeForward = 0, kModeCentral = 1, kModeBinary = 2 };
+
+namespace {
+
+struct TraverseSmem {
+    uint64_t edge[256];
+    uint32_t codew[kWarps][kBlockWords];
+    uint16_t pref[kWarps][kBlockKeys];
+    uint32_t top[kTopCacheEntries];
+    uint8_t cnt[256];
+};
+
+__device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        S.cnt[i] = c_vertex_count_t[i];
+        S.edge[i] = c_edge_nibbles[i];
+    }
+    for (int i = threadIdx.x; i < V.top_cached; i += blockDim.x) S.top[i] = V.levels[i];
+    __syncthreads();
+}
+
+// Descent through the dense levels (jtop-1 .. 5) for vertex key v.
+__device__ __forceinline__ void descend(const Volume& V, const TraverseSmem& S, unsigned long long v,
+                                        unsigned long long& block, unsigned long long& base,
+                                        unsigned int& count) {
+    unsigned long long node = 0, key = v;
+    base = 0;
+    count = V.levels[V.level_off[V.jtop]];
+    for (int j = V.jtop - 1; j >= kBlockLevel; j--) {
+        const long long idx = V.level_off[j] + 4ll * (long long)node;
+        uint4 s;
+        if (idx + 4 <= V.top_cached)
+            s = *reinterpret_cast<const uint4*>(&S.top[idx]);
+        else
+            s = __ldg(reinterpret_cast<const uint4*>(V.levels + idx));
+        const unsigned long long s0 = s.x, s1 = s0 + s.y, s2 = s1 + s.z;
+        unsigned long long skip;
+        unsigned int c, cnt;
+        if (key < s0) {
+            c = 0; skip = 0; cnt = s.x;
+        } else if (key < s1) {
+            c = 1; skip = s0; cnt = s.y;
+        } else if (key < s2) {
+            c = 2; skip = s1; cnt = s.z;
+        } else {
+            c = 3; skip = s2; cnt = s.w;
+        }
+        key -= skip;
+        base += skip;
+        node = 4ull * node + c;
+        count = cnt;
+    }
+    block = node;
+}
+
+// Warp-cooperative: per-cell inclusive prefix of vertex counts of block b.
+__device__ __forceinline__ void load_block(const Volume& V, TraverseSmem& S, int warp, int lane,
+                                           unsigned long long b) {
+    const long long slot = block_slot(V, b);
+    const uint4* src = reinterpret_cast<const uint4*>(V.arena + slot * kBlockWords) + 2 * lane;
+    const uint4 w0 = __ldg(src), w1 = __ldg(src + 1);
+    const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    uint32_t run = 0;
+    uint32_t incl[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        run += S.cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        incl[i] = run;
+    }
+    // exclusive scan of the lane sums
+    uint32_t scan = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
+        if (lane >= o) scan += t;
+    }
+    const uint32_t excl = scan - run;
+    uint32_t* pref32 = reinterpret_cast<uint32_t*>(&S.pref[warp][32 * lane]);
+#pragma unroll
+    for (int i = 0; i < 16; i++) pref32[i] = (excl + incl[2 * i]) | ((excl + incl[2 * i + 1]) << 16);
+    uint4* cw = reinterpret_cast<uint4*>(&S.codew[warp][8 * lane]);
+    cw[0] = w0;
+    cw[1] = w1;
+    __syncwarp();
+}
+
+// Resolved vertex: cell, code, vertex index inside the cell.
+struct VertexCell {
+    int x, y, z;
+    int code;
+    int k;
+};
+
+__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp,
+                                                unsigned long long b, unsigned int key) {
+    const uint16_t* pref = S.pref[warp];
+    int lo = 0;
+#pragma unroll
+    for (int step = 512; step >= 1; step >>= 1)
+        if (pref[lo + step - 1] <= key) lo += step;
+    VertexCell r;
+    r.code = (S.codew[warp][lo >> 2] >> (8 * (lo & 3))) & 0xff;
+    r.k = (int)key - ((int)pref[lo] - (int)S.cnt[r.code]);
+    r.k = min(max(r.k, 0), 15);  // in range whenever key < block count (table reads stay in bounds)
+    int cx, cy;
+    morton10((uint32_t)lo, cx, cy);
+    const uint32_t X = (morton_compact(b) << 5) + (uint32_t)cx;
+    const uint32_t Y = (morton_compact(b >> 1) << 5) + (uint32_t)cy;
+    virtual_to_cell(V, X, Y, r.x, r.y, r.z);
+    return r;
+}
+
+// Steps 1-2 for one round of 32 vertices of a warp; returns false for lanes
+// without a vertex.  (bb, bbase, bcount) is the warp's cached block.
+__device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S, int warp, int lane,
+                                               unsigned long long v, bool act, long long& bb,
+                                               unsigned long long& bbase, unsigned int& bcount,
+                                               VertexCell& out) {
+    unsigned long long myb = (unsigned long long)bb, mybase = bbase;
+    unsigned int mycnt = bcount;
+    const bool cached = bb >= 0 && v >= bbase && v < bbase + bcount;
+    if (act && !cached) descend(V, S, v, myb, mybase, mycnt);
+    unsigned int pending = __ballot_sync(0xffffffffu, act);
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const unsigned long long lb = __shfl_sync(0xffffffffu, myb, leader);
+        if ((long long)lb != bb) {
+            bbase = __shfl_sync(0xffffffffu, mybase, leader);
+            bcount = __shfl_sync(0xffffffffu, mycnt, leader);
+            bb = (long long)lb;
+            load_block(V, S, warp, lane, lb);
+        }
+        const bool mine = ((pending >> lane) & 1u) && myb == (unsigned long long)bb;
+        if (mine) out = find_cell(V, S, warp, (unsigned long long)bb, (unsigned int)(v - bbase));
+        pending &= ~__ballot_sync(0xffffffffu, mine);
+        __syncwarp();
+    }
+    return act;
+}
+
+struct EdgeGeom {
+    int a[3];
+    int axis;
+    int edge;
+};
+
+__device__ __forceinline__ EdgeGeom edge_of(const TraverseSmem& S, const VertexCell& c) {
+    EdgeGeom g;
+    g.edge = (int)((S.edge[c.code] >> (4 * c.k)) & 15ull);
+    const uint32_t e = (uint32_t)(kEdgeGeometry >> (5 * g.edge)) & 31u;
+    g.a[0] = c.x + (int)(e & 1u);
+    g.a[1] = c.y + (int)((e >> 1) & 1u);
+    g.a[2] = c.z + (int)((e >> 2) & 1u);
+    g.axis = (int)(e >> 3);
+    return g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+template <int FT, int MODE>
+__global__ void __launch_bounds__(kThreads) traverse_kernel(const __grid_constant__ Volume V,
+                                                            const __grid_constant__ TraverseOut O) {
+    __shared__ __align__(16) TraverseSmem S;
+    load_tables(V, S);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long total = V.ctrl->total;
+    const unsigned long long N = total < O.capacity ? total : O.capacity;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (total > O.capacity) atomicOr(&V.ctrl->status, kStatusCapacity);
+        V.ctrl->written = (unsigned int)N;
+    }
+    const float iso = V.iso;
+    constexpr unsigned long long VW = 32ull * kTraverseRounds;
+    const unsigned long long nchunks = (N + VW - 1) / VW;
+    long long bb = -1;
+    unsigned long long bbase = 0;
+    unsigned int bcount = 0;
+    for (unsigned long long chunk = (unsigned long long)blockIdx.x * kWarps + warp; chunk < nchunks;
+         chunk += (unsigned long long)gridDim.x * kWarps) {
+#pragma unroll 1
+        for (int r = 0; r < kTraverseRounds; r++) {
+            const unsigned long long v = chunk * VW + 32ull * r + lane;
+            const bool act = v < N;
+            if (!__any_sync(0xffffffffu, act)) break;
+            VertexCell c;
+            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, c)) continue;
+            const EdgeGeom g = edge_of(S, c);
+            const int ax = g.axis;
+            float t, n[3];
+            if (MODE == kModeBinary) {
+                t = 0.5f;
+                const float* bn = g_binary_normals + 3 * (16 * c.code + c.k);
+                n[0] = bn[0]; n[1] = bn[1]; n[2] = bn[2];
+            } else {
+                const int* a = g.a;
+                const int b[3] = {a[0] + (ax == 0), a[1] + (ax == 1), a[2] + (ax == 2)};
+                const float va = fetch<FT>(V, a[0], a[1], a[2]);
+                const float vb = fetch<FT>(V, b[0], b[1], b[2]);
+                t = (va - iso) / (va - vb);
+                const float omt = 1.0f - t;
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const int ex = (i == 0), ey = (i == 1), ez = (i == 2);
+                    const float fa_p = (i == ax) ? vb : fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
+                    const float fb_p = fetch<FT>(V, b[0] + ex, b[1] + ey, b[2] + ez);
+                    if (MODE == kModeForward) {
+                        // iso - lerp(f(a+e), f(b+e), t), differences first
+                        n[i] = omt * (iso - fa_p) + t * (iso - fb_p);
+                    } else {
+                        const float fa_m = fetch<FT>(V, a[0] - ex, a[1] - ey, a[2] - ez);
+                        const float fb_m = (i == ax) ? va : fetch<FT>(V, b[0] - ex, b[1] - ey, b[2] - ez);
+                        n[i] = -0.5f * (omt * (fa_p - fa_m) + t * (fb_p - fb_m));
+                    }
+                }
+            }
+            float p[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                p[i] = ((float)g.a[i] + (i == ax ? t : 0.0f)) * V.scale[i];
+                n[i] *= V.scale[i];
+            }
+            const unsigned long long o = V.vertex_base + v;
+            if (O.pos) __stcs(O.pos + o, make_float4(p[0], p[1], p[2], 1.0f));
+            if (O.nrm) __stcs(O.nrm + o, make_float4(n[0], n[1], n[2], 0.0f));
+            if (O.feedback) {
+                float2* fb = reinterpret_cast<float2*>(O.feedback + 6ull * o);
+                __stcs(fb + 0, make_float2(n[0], n[1]));
+                __stcs(fb + 1, make_float2(n[2], p[0]));
+                __stcs(fb + 2, make_float2(p[1], p[2]));
+            }
+            if (O.dbg_cell) O.dbg_cell[o] = make_int4(c.x, c.y, c.z, c.code | (c.k << 8) | (g.edge << 16));
+            if (O.dbg_t) O.dbg_t[o] = t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: recompute the traversal of each vertex and scatter
+// dL/dp . dp/df + dL/dn . dn/df onto the field samples the vertex read.
+//   t = (f_a - iso)/(f_a - f_b):  dt/df_a = (iso - f_b)/(f_a - f_b)^2,
+//                                 dt/df_b = (f_a - iso)/(f_a - f_b)^2
+//   p_axis = (a_axis + t) s_axis
+//   forward: n_i = ((1-t)(iso - f(a+e_i)) + t(iso - f(b+e_i))) s_i
+//   central: n_i = -1/2((1-t)(f(a+e_i) - f(a-e_i)) + t(f(b+e_i) - f(b-e_i))) s_i
+// Clamped samples scatter to the sample that was read.
+namespace {
+template <int FT>
+__device__ __forceinline__ void scatter(const Volume& V, float* dfield, int x, int y, int z, float g) {
+    x = min(max(x, 0), V.lattice[0] - 1);
+    y = min(max(y, 0), V.lattice[1] - 1);
+    z = min(max(z, 0), V.lattice[2] - 1);
+    atomicAdd(dfield + (long long)z * V.slice_pitch + (long long)y * V.row_pitch + x, g);
+}
+}  // namespace
+
+template <int FT, int MODE>
+__global__ void __launch_bounds__(kThreads) adjoint_kernel(const __grid_constant__ Volume V,
+                                                           const __grid_constant__ AdjointIO A) {
+    __shared__ __align__(16) TraverseSmem S;
+    load_tables(V, S);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long total = V.ctrl->total;
+    const unsigned long long N = total < A.count ? total : A.count;
+    const float iso = V.iso;
+    constexpr unsigned long long VW = 32ull * kTraverseRounds;
+    const unsigned long long nchunks = (N + VW - 1) / VW;
+    long long bb = -1;
+    unsigned long long bbase = 0;
+    unsigned int bcount = 0;
+    for (unsigned long long chunk = (unsigned long long)blockIdx.x * kWarps + warp; chunk < nchunks;
+         chunk += (unsigned long long)gridDim.x * kWarps) {
+#pragma unroll 1
+        for (int r = 0; r < kTraverseRounds; r++) {
+            const unsigned long long v = chunk * VW + 32ull * r + lane;
+            const bool act = v < N;
+            if (!__any_sync(0xffffffffu, act)) break;
+            VertexCell c;
+            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, c)) continue;
+            const EdgeGeom g = edge_of(S, c);
+            const int ax = g.axis;
+            const int* a = g.a;
+            const int b[3] = {a[0] + (ax == 0), a[1] + (ax == 1), a[2] + (ax == 2)};
+            const unsigned long long o = V.vertex_base + v;
+            const float4 dp = A.dpos ? __ldg(A.dpos + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 dn = A.dnrm ? __ldg(A.dnrm + o) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float dpv[3] = {dp.x, dp.y, dp.z};
+            const float dnv[3] = {dn.x * V.scale[0], dn.y * V.scale[1], dn.z * V.scale[2]};
+            const float va = fetch<FT>(V, a[0], a[1], a[2]);
+            const float vb = fetch<FT>(V, b[0], b[1], b[2]);
+            const float den = va - vb;
+            const float t = (va - iso) / den;
+            const float omt = 1.0f - t;
+            float dLdt = dpv[ax] * V.scale[ax];
+            float ga = 0.0f, gb = 0.0f;  // direct contributions to samples a and b
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int ex = (i == 0), ey = (i == 1), ez = (i == 2);
+                const float fa_p = (i == ax) ? vb : fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
+                const float fb_p = fetch<FT>(V, b[0] + ex, b[1] + ey, b[2] + ez);
+                if (MODE == kModeForward) {
+                    dLdt += dnv[i] * (fa_p - fb_p);
+                    const float wa = -omt * dnv[i], wb = -t * dnv[i];
+                    if (i == ax) gb += wa; else scatter<FT>(V, A.dfield, a[0] + ex, a[1] + ey, a[2] + ez, wa);
+                    scatter<FT>(V, A.dfield, b[0] + ex, b[1] + ey, b[2] + ez, wb);
+                } else {
+                    const float fa_m = fetch<FT>(V, a[0] - ex, a[1] - ey, a[2] - ez);
+                    const float fb_m = (i == ax) ? va : fetch<FT>(V, b[0] - ex, b[1] - ey, b[2] - ez);
+                    dLdt += -0.5f * dnv[i] * ((fb_p - fb_m) - (fa_p - fa_m));
+                    const float wa = -0.5f * omt * dnv[i], wb = -0.5f * t * dnv[i];
+                    if (i == ax) gb += wa; else scatter<FT>(V, A.dfield, a[0] + ex, a[1] + ey, a[2] + ez, wa);
+                    scatter<FT>(V, A.dfield, a[0] - ex, a[1] - ey, a[2] - ez, -wa);
+                    scatter<FT>(V, A.dfield, b[0] + ex, b[1] + ey, b[2] + ez, wb);
+                    if (i == ax) ga -= wb; else scatter<FT>(V, A.dfield, b[0] - ex, b[1] - ey, b[2] - ez, -wb);
+                }
+            }
+            const float inv = 1.0f / (den * den);
+            ga += dLdt * (iso - vb) * inv;
+            gb += dLdt * (va - iso) * inv;
+            scatter<FT>(V, A.dfield, a[0], a[1], a[2], ga);
+            scatter<FT>(V, A.dfield, b[0], b[1], b[2], gb);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
+                            cudaStream_t st) {
+    const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
+#define HPMC_TRAVERSE_CASE(FT_)                                                                   \
+    case FT_:                                                                                     \
+        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, 0, st>>>(V, O); \
+        else if (mode == kModeCentral) traverse_kernel<FT_, kModeCentral><<<grid, kThreads, 0, st>>>(V, O); \
+        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, 0, st>>>(V, O);                \
+        break;
+    switch (V.ftype) {
+        HPMC_TRAVERSE_CASE(kFieldF32)
+        HPMC_TRAVERSE_CASE(kFieldU8)
+        HPMC_TRAVERSE_CASE(kFieldUNorm8)
+        HPMC_TRAVERSE_CASE(kFieldFunctor)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HPMC_TRAVERSE_CASE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode, int grid, cudaStream_t st) {
+    const bool central = normal_mode == kNormalsCentral;
+    switch (V.ftype) {
+        case kFieldF32:
+            if (central) adjoint_kernel<kFieldF32, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
+            else adjoint_kernel<kFieldF32, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            break;
+        case kFieldU8:
+            if (central) adjoint_kernel<kFieldU8, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
+            else adjoint_kernel<kFieldU8, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            break;
+        case kFieldUNorm8:
+            if (central) adjoint_kernel<kFieldUNorm8, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
+            else adjoint_kernel<kFieldUNorm8, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace hpmc
+
+namespace hpmc {
+
+int traverse_blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<kFieldF32, kModeCentral>, kThreads, 0) !=
+            cudaSuccess ||
+        n < 1)
+        n = 1;
+    return n;
+}
+
+}  // namespace hpmc

@@ -1,0 +1,247 @@
+/*
+ * hpmc.h -- C ABI of the B200-native HistoPyramid marching-cubes extractor.
+ *
+ * Drop-in for HPMC's public interface (hpmc/include/hpmc.h:291-549 of the
+ * reference, "extern C", opaque handles): every reference entry point keeps
+ * its name, argument list and error convention (NULL / false / 0 returns and a
+ * sticky "broken" flag on the pyramid handle).  The GL context leaves the hot
+ * path: fields are device arrays or registered device functors, the pyramid
+ * lives in device memory, and traversal writes vertices into caller-owned
+ * device buffers instead of a GL draw or transform feedback.  The extra entry
+ * points below the reference block are CUDA-native; each returns an
+ * HPMCStatus.  Handles are not thread-safe; distinct handles are independent.
+ *
+ * Scalar types come from hpmc_types.h (GL's widths, no GL header needed).
+ */
+#ifndef HPMC_B200_H
+#define HPMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "hpmc_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#else
+#include <stdbool.h>
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+struct HPMCConstants;
+struct HPMCHistoPyramid;
+struct HPMCTraversalHandle;
+
+/* ---- status codes (HPMCgetLastError and the CUDA-native entry points) ---- */
+typedef enum HPMCStatus {
+    HPMC_OK = 0,
+    HPMC_ERR_INVALID_HANDLE = 1,  /* NULL or destroyed handle */
+    HPMC_ERR_INVALID_VALUE = 2,   /* bad argument */
+    HPMC_ERR_LAYOUT = 3,          /* lattice/grid sizes rejected (init.cpp:82-103) */
+    HPMC_ERR_UNSUPPORTED = 4,     /* GL/GLSL-only feature with no device equivalent */
+    HPMC_ERR_CUDA = 5,            /* a CUDA call failed */
+    HPMC_ERR_OUT_OF_MEMORY = 6,
+    HPMC_ERR_CAPACITY = 7,        /* output buffer smaller than the vertex count */
+    HPMC_ERR_NOT_BUILT = 8,       /* extraction before HPMCbuildHistopyramid */
+    HPMC_ERR_BROKEN = 9,          /* handle is broken until reconfigured */
+    HPMC_ERR_NO_FIELD = 10,       /* no field source set */
+    HPMC_ERR_OVERFLOW = 11,       /* vertex count does not fit 32 bits */
+    HPMC_ERR_TIMEOUT = 12         /* a bounded device wait gave up */
+} HPMCStatus;
+
+/* ---- field element types of device arrays ---- */
+typedef enum HPMCScalarType {
+    HPMC_SCALAR_F32 = 0,     /* float */
+    HPMC_SCALAR_U8 = 1,      /* uint8 read as float(b) */
+    HPMC_SCALAR_UNORM8 = 2   /* uint8 read as b/255, like a GL_ALPHA / GL_UNSIGNED_BYTE texture */
+} HPMCScalarType;
+
+/* ---- normal estimation ---- */
+typedef enum HPMCNormalMode {
+    HPMC_NORMALS_FORWARD = 0,  /* reference: iso - lerp(f(a+e_i), f(b+e_i), t) (shadergen.cpp:528-551) */
+    HPMC_NORMALS_CENTRAL = 1   /* -lerp(central difference at a, at b, t) / 2 steps, same scaling */
+} HPMCNormalMode;
+
+/* ======================= reference entry points ========================= */
+
+/* hpmc.h:310-311 / constants.cpp:54-347.  Device-side constant tables for
+ * the current CUDA device.  NULL if no CUDA device is usable or if
+ * max_gl_major < 2 (the reference's "GL 2.0 required" rejection). */
+struct HPMCConstants* HPMCcreateConstants(GLint max_gl_major, GLint max_gl_minor);
+
+/* hpmc.h:319-320 / constants.cpp:350-392.  NULL-safe. */
+void HPMCdestroyConstants(struct HPMCConstants* c);
+
+/* hpmc.h:330-331 / hpiface.cpp:45-97.  NULL if constants is NULL.  Starts
+ * broken until a lattice/grid/field setter is called (hpiface.cpp:57). */
+struct HPMCHistoPyramid* HPMCcreateHistoPyramid(struct HPMCConstants* s);
+
+/* hpmc.h:345-349 / hpiface.cpp:100-114.  cells := size - 1; taints. */
+void HPMCsetLatticeSize(struct HPMCHistoPyramid* h, GLsizei x_size, GLsizei y_size, GLsizei z_size);
+
+/* hpmc.h:351-352 / hpiface.cpp:131-135.  Threshold 0.5, edge midpoints and
+ * table normals.  Does not taint (as in the reference). */
+void HPMCsetFieldAsBinary(struct HPMCHistoPyramid* h);
+
+/* hpmc.h:354-355 / hpiface.cpp:138-142. */
+void HPMCsetFieldAsContinuous(struct HPMCHistoPyramid* h);
+
+/* hpmc.h:374-378 / hpiface.cpp:117-128.  Checked lazily (init.cpp:98-103). */
+void HPMCsetGridSize(struct HPMCHistoPyramid* h, GLsizei x_size, GLsizei y_size, GLsizei z_size);
+
+/* hpmc.h:391-395 / hpiface.cpp:145-161.  Default (1,1,1). */
+void HPMCsetGridExtent(struct HPMCHistoPyramid* h, GLfloat x_extent, GLfloat y_extent, GLfloat z_extent);
+
+/* hpmc.h:404-407 / hpiface.cpp:164-184.  `texture` is a field name returned
+ * by HPMCregisterDeviceField (the stand-in for a GL 3-D texture name);
+ * gradient must be GL_FALSE (gradient lattices: HPMC_ERR_UNSUPPORTED). */
+void HPMCsetFieldTexture3D(struct HPMCHistoPyramid* h, GLuint texture, GLboolean gradient);
+
+/* hpmc.h:440-444 / hpiface.cpp:187-200.  shader_source names a registered
+ * device functor instead of carrying GLSL: "hpmc:cayley",
+ * "hpmc:metaballs", "hpmc:twist_metaballs", "hpmc:spheres".  Any other text
+ * sets HPMC_ERR_UNSUPPORTED and breaks the handle.  builder_texunit is
+ * ignored.  gradient = GL_TRUE uses the functor's analytic gradient for
+ * normals where it has one (cayley). */
+void HPMCsetFieldCustom(struct HPMCHistoPyramid* h, const char* shader_source, GLuint builder_texunit,
+                        GLboolean gradient);
+
+/* hpmc.h:446-447 / hpiface.cpp:202-222.  Returns a non-zero parameter-block
+ * name for the functor's uniforms (set them with HPMCsetBuilderUniforms), 0
+ * if the handle is broken. */
+GLuint HPMCgetBuilderProgram(struct HPMCHistoPyramid* h);
+
+/* hpmc.h:451-452 (declared, never defined by the reference).  Destroys the
+ * pyramid and its device memory; NULL-safe. */
+void HPMCdestroyHandle(struct HPMCHistoPyramid* handle);
+
+/* hpmc.h:460-462 / hpiface.cpp:225-290.  Classifies the field at `threshold`
+ * and builds the pyramid on the handle's stream (asynchronous).  Errors set
+ * the broken flag. */
+void HPMCbuildHistopyramid(struct HPMCHistoPyramid* h, GLfloat threshold);
+
+/* hpmc.h:468-469 / hpiface.cpp:293-345.  Vertex count of the last build;
+ * waits for it (host sync).  0 on error or if the count exceeds 32 bits. */
+GLuint HPMCacquireNumberOfVertices(struct HPMCHistoPyramid* handle);
+
+/* hpmc.h:478-479 / triface.cpp:43-109.  NULL if the pyramid cannot be set up. */
+struct HPMCTraversalHandle* HPMCcreateTraversalHandle(struct HPMCHistoPyramid* handle);
+
+/* hpmc.h:485-486 / triface.cpp:112-122. */
+void HPMCdestroyTraversalHandle(struct HPMCTraversalHandle* th);
+
+/* hpmc.h:495-496 / triface.cpp:125-192.  There is no GLSL to hand out:
+ * returns NULL and sets HPMC_ERR_UNSUPPORTED. */
+char* HPMCgetTraversalShaderFunctions(struct HPMCTraversalHandle* th);
+
+/* hpmc.h:516-521 / triface.cpp:195-327.  No GL program exists: returns false
+ * and sets HPMC_ERR_UNSUPPORTED.  Bind output buffers with
+ * HPMCsetTraversalHandleBuffers instead. */
+bool HPMCsetTraversalHandleProgram(struct HPMCTraversalHandle* th, GLuint program, GLuint tex_unit_work1,
+                                   GLuint tex_unit_work2, GLuint tex_unit_work3);
+
+/* hpmc.h:534-535 / triface.cpp:460-464.  Writes every vertex of the last
+ * build into the buffers bound by HPMCsetTraversalHandleBuffers (float4
+ * positions and normals).  false if no buffers are bound, the pyramid is
+ * broken or the buffers are too small (the first `capacity` vertices are
+ * written and HPMC_ERR_CAPACITY is set). */
+bool HPMCextractVertices(struct HPMCTraversalHandle* th);
+
+/* hpmc.h:537-544 / triface.cpp:468-500.  Transform-feedback capture: writes
+ * interleaved N3F_V3F (normal xyz, position xyz) into the buffer bound by
+ * HPMCsetTraversalHandleFeedbackBuffer.  The NV and EXT variants are the same
+ * call. */
+bool HPMCextractVerticesTransformFeedback(struct HPMCTraversalHandle* th);
+bool HPMCextractVerticesTransformFeedbackNV(struct HPMCTraversalHandle* th);
+bool HPMCextractVerticesTransformFeedbackEXT(struct HPMCTraversalHandle* th);
+
+/* ===================== CUDA-native entry points ========================= */
+
+/* Last status of a pyramid handle (cleared by a successful reconfiguration). */
+int HPMCgetLastError(struct HPMCHistoPyramid* h);
+
+/* Stand-in for glTexImage3D + a texture name: registers a device array as a
+ * field and returns its non-zero name for HPMCsetFieldTexture3D (0 on bad
+ * arguments).  Pitches in bytes; 0 means dense.  The array is not copied. */
+GLuint HPMCregisterDeviceField(const void* device_ptr, int scalar_type, GLsizei x_size, GLsizei y_size,
+                               GLsizei z_size, size_t row_pitch_bytes, size_t slice_pitch_bytes);
+void HPMCunregisterDeviceField(GLuint name);
+
+/* Sets a device array as the field directly (lattice size from
+ * HPMCsetLatticeSize).  Pitches in bytes, 0 = dense.  Taints the handle. */
+int HPMCsetFieldDevice(struct HPMCHistoPyramid* h, const void* device_ptr, int scalar_type,
+                       size_t row_pitch_bytes, size_t slice_pitch_bytes);
+
+/* Uniform values of a functor field (glUniform on the builder program in
+ * the reference's custom-fetch use, apps/metaballs/metaballs.cpp:277-281). */
+int HPMCsetBuilderUniforms(struct HPMCHistoPyramid* h, const float* values, int count);
+
+/* CUDA stream all work of this handle is issued on (default: stream 0). */
+int HPMCsetStream(struct HPMCHistoPyramid* h, void* cuda_stream);
+
+/* Normal estimation (default HPMC_NORMALS_FORWARD, the reference's). */
+int HPMCsetNormalMode(struct HPMCHistoPyramid* h, int mode);
+
+/* Device-side vertex count of the last build (uint64, device pointer) for
+ * stream-ordered consumers; valid after the build completes on the stream. */
+int HPMCgetDeviceVertexCount(struct HPMCHistoPyramid* h, const unsigned long long** device_count);
+
+/* Output buffers used by HPMCextractVertices (device pointers; float4 x,y,z,1
+ * and nx,ny,nz,0 per vertex; either may be NULL) and their capacity. */
+int HPMCsetTraversalHandleBuffers(struct HPMCTraversalHandle* th, float* positions, float* normals,
+                                  size_t capacity_vertices);
+
+/* Output buffer of HPMCextractVerticesTransformFeedback*: 6 floats per vertex. */
+int HPMCsetTraversalHandleFeedbackBuffer(struct HPMCTraversalHandle* th, float* n3f_v3f,
+                                         size_t capacity_vertices);
+
+/* One-call extraction into device buffers without a host sync: the kernel
+ * reads the vertex count on the device.  If n_written is non-NULL the call
+ * waits and stores the number of vertices written. */
+int HPMCextractVerticesToBuffers(struct HPMCTraversalHandle* th, float* positions, float* normals,
+                                 size_t capacity_vertices, uint64_t* n_written);
+
+/* Adjoint of the extraction: given dL/dp and dL/dn per vertex (float4, w
+ * ignored; either may be NULL) for the first `count` vertices of the last
+ * build, ACCUMULATES dL/df into d_field, a float array with the field's
+ * lattice shape and element pitches (dense when the field is dense).
+ * Recomputes the traversal; topology is piecewise constant.  F32/U8/UNORM8
+ * array fields, forward or central normals; binary fields have zero
+ * gradient. */
+int HPMCextractVerticesAdjoint(struct HPMCTraversalHandle* th, const float* dL_dpositions,
+                               const float* dL_dnormals, uint64_t count, float* d_field);
+
+/* ---- inspection (tests, tools) ---- */
+
+/* Capture every cell's MC code during the next builds into a device buffer
+ * of cells_x*cells_y*cells_z bytes ([z][y][x]); NULL stops capturing. */
+int HPMCsetCodeCapture(struct HPMCHistoPyramid* h, uint8_t* device_codes);
+
+/* Layout of the pyramid: out[0..5] = tile_x, tile_y, layout_x, layout_y,
+ * size_l2, size (init.cpp:105-130). */
+int HPMCgetLayout(struct HPMCHistoPyramid* h, int out[6]);
+
+/* Copies dense pyramid level j (5 <= j <= size_l2 + 1, the reference's mip
+ * level j flattened channel-wise in Morton order; entries = 4^(size_l2+1-j))
+ * into host memory. */
+int HPMCreadLevel(struct HPMCHistoPyramid* h, int level, uint32_t* host_out, size_t entries);
+
+/* Per-vertex debug outputs of the next extractions (device pointers, may be
+ * NULL): int4 (x, y, z, code | k << 8 | edge << 16) and float t. */
+int HPMCsetTraversalDebugBuffers(struct HPMCTraversalHandle* th, int32_t* cell_info, float* t);
+
+/* Device status word of the pyramid (bits: 1 overflow, 2 capacity,
+ * 4 arena, 8 timeout); waits for the handle's stream. */
+int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,202 @@
+"""CUDA path vs the oracle through the C ABI (needs a B200).
+
+Topology (case indices, every dense pyramid level, the vertex count and the
+vertex -> (cell, k, edge) order) must be bit-exact.  Geometry: the edge
+parameter t within 1e-5 (cell-local), positions within 1e-5 of the lattice
+spacing plus 4 FP32 ulps of the world coordinate, normals within 1e-5 rad of
+the FP64 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from tests.golden import make_golden
+from tests.gpu_helpers import compare, oracle_expect, run_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", sorted(make_golden.CASES))
+@pytest.mark.parametrize("normals", [0, 1])
+def test_golden_cases(hpmc, oracle, name, normals):
+    case = make_golden.CASES[name]
+    field = make_golden.make_field(case["kind"], case["shape"], case["seed"])
+    kw = dict(cells=case.get("cells"), extent=case.get("extent", (1.0, 1.0, 1.0)),
+              binary=case.get("binary", False), unorm=case.get("unorm", False))
+    g = run_gpu(hpmc, field, case["iso"], normals=normals, **kw)
+    e = oracle_expect(oracle, field, case["iso"], normals=normals, **kw)
+    compare(g, e, extent=kw["extent"], binary=kw["binary"])
+    # the committed fixtures agree with both
+    gold = np.load(__import__("os").path.join(make_golden.HERE, name + ".npz"))
+    assert int(gold["total"][0]) == g["n"]
+    assert np.array_equal(gold["cell"], g["info"][:, :3])
+
+
+SHAPES = [(3, 3, 3), (4, 5, 6), (9, 9, 9), (5, 7, 9), (40, 3, 21), (17, 33, 12), (33, 33, 33), (34, 65, 66),
+          (70, 40, 100), (64, 64, 64), (48, 128, 36)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("dtype", ["f32", "u8"])
+def test_random_lattices(hpmc, oracle, shape, dtype):
+    rng = np.random.default_rng(sum(shape) * 7 + (0 if dtype == "f32" else 1000))
+    if dtype == "f32":
+        field = rng.normal(size=shape).astype(np.float32)
+        field[rng.random(shape) < 0.05] = 0.0  # exact ties with iso 0
+        iso = 0.0
+    else:
+        field = rng.integers(100, 156, size=shape).astype(np.uint8)
+        iso = 128.0
+    g = run_gpu(hpmc, field, iso)
+    e = oracle_expect(oracle, field, iso)
+    compare(g, e)
+
+
+@pytest.mark.parametrize("pad", [1, 3, 16])
+def test_pitched_fields_take_generic_path_identically(hpmc, oracle, pad):
+    rng = np.random.default_rng(pad)
+    field = rng.normal(size=(40, 36, 70)).astype(np.float32)
+    g = run_gpu(hpmc, field, 0.1, pitch_pad=pad)
+    e = oracle_expect(oracle, field, 0.1)
+    compare(g, e)
+
+
+def test_grid_smaller_than_lattice(hpmc, oracle):
+    rng = np.random.default_rng(5)
+    field = rng.normal(size=(30, 50, 70)).astype(np.float32)
+    cells = (50, 40, 20)
+    g = run_gpu(hpmc, field, 0.0, cells=cells, extent=(1.0, 2.0, 3.0))
+    e = oracle_expect(oracle, field, 0.0, cells=cells, extent=(1.0, 2.0, 3.0))
+    compare(g, e, extent=(1.0, 2.0, 3.0))
+
+
+def test_config_metaballs_64(hpmc, oracle):
+    from hpmc_b200 import datasets
+
+    field, iso = datasets.metaballs_64()
+    for normals in (0, 1):
+        g = run_gpu(hpmc, field, iso, normals=normals)
+        e = oracle_expect(oracle, field, iso, normals=normals)
+        rep = compare(g, e)
+        assert rep["n"] > 50000
+
+
+def test_config_spheres_128(hpmc, oracle):
+    from hpmc_b200 import datasets
+
+    field, iso = datasets.spheres_sdf()
+    g = run_gpu(hpmc, field, iso, normals=1)
+    e = oracle_expect(oracle, field, iso, normals=1)
+    compare(g, e)
+
+
+@pytest.mark.slow
+def test_config_noise_u8_256_ties(hpmc, oracle):
+    """uint8 256^3 with ~256k samples equal to the iso-value: >2^24 vertices."""
+    from hpmc_b200 import datasets
+
+    field, iso = datasets.noise_u8()
+    assert int((field == 128).sum()) > 100000
+    g = run_gpu(hpmc, field, iso, normals=1)
+    e = oracle_expect(oracle, field, iso, normals=1)
+    rep = compare(g, e)
+    assert rep["n"] > 2**24
+
+
+def test_binary_mode_and_feedback_capture(hpmc, oracle):
+    """Binary fields (midpoints + table normals) and the N3F_V3F capture."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    field = rng.random((20, 22, 24)).astype(np.float32)
+    g = run_gpu(hpmc, field, 0.0, binary=True)
+    e = oracle_expect(oracle, field, 0.0, binary=True)
+    compare(g, e, binary=True)
+    # transform-feedback layout through the reference entry point
+    dev = torch.device("cuda:0")
+    t = torch.from_numpy(field).to(dev)
+    hp = hpmc.HistoPyramid(hpmc.default_constants())
+    hp.set_stream(torch.cuda.current_stream())
+    hp.set_field_device(t)
+    hp.set_field_as_binary()
+    hp.build(0.0)
+    n = hp.acquire_number_of_vertices()
+    th = hpmc.TraversalHandle(hp)
+    fb = torch.zeros(n * 6, dtype=torch.float32, device=dev)
+    th.set_feedback_buffer(fb, n)
+    assert th.extract_feedback()
+    torch.cuda.synchronize()
+    fb = fb.cpu().numpy().reshape(n, 6)
+    np.testing.assert_array_equal(fb[:, 3:], g["pos"][:, :3])
+    np.testing.assert_array_equal(fb[:, :3], g["nrm"][:, :3])
+
+
+def test_reference_call_sequence_and_errors(hpmc):
+    """The reference's API sequence (texture3d app, apps/texture3d/texture3d.cpp:144-221)
+    with a registered device field standing in for the GL texture."""
+    import ctypes as C
+
+    import torch
+
+    from hpmc_b200 import _capi
+
+    L = hpmc.lib()
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(1)
+    vol = torch.from_numpy(rng.integers(0, 255, size=(24, 20, 16)).astype(np.uint8)).to(dev)
+    c = L.HPMCcreateConstants(4, 3)
+    assert c
+    h = L.HPMCcreateHistoPyramid(c)
+    assert L.HPMCacquireNumberOfVertices(h) == 0  # broken until configured (hpiface.cpp:57)
+    name = L.HPMCregisterDeviceField(vol.data_ptr(), _capi.SCALAR_UNORM8, 16, 20, 24, 0, 0)
+    L.HPMCsetLatticeSize(h, 16, 20, 24)
+    L.HPMCsetGridSize(h, 15, 19, 23)
+    L.HPMCsetGridExtent(h, 16 / 24, 20 / 24, 1.0)
+    L.HPMCsetFieldTexture3D(h, name, 0)
+    th = L.HPMCcreateTraversalHandle(h)
+    assert th
+    assert L.HPMCgetTraversalShaderFunctions(th) is None
+    assert L.HPMCgetLastError(h) == _capi.ERR_UNSUPPORTED
+    assert L.HPMCsetTraversalHandleProgram(th, 1, 0, 1, 2) is False
+    assert L.HPMCextractVertices(th) is False  # no output buffers bound
+    L.HPMCbuildHistopyramid(h, 0.5)
+    n = L.HPMCacquireNumberOfVertices(h)
+    assert n > 0
+    pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    assert L.HPMCsetTraversalHandleBuffers(th, pos.data_ptr(), nrm.data_ptr(), n) == 0
+    assert L.HPMCextractVertices(th) is True
+    # too-small buffers: first `capacity` vertices written, HPMC_ERR_CAPACITY reported
+    small = torch.full((5, 4), -7.0, dtype=torch.float32, device=dev)
+    assert L.HPMCsetTraversalHandleBuffers(th, small.data_ptr(), None, 5) == 0
+    assert L.HPMCextractVertices(th) is False
+    assert L.HPMCgetLastError(h) == _capi.ERR_CAPACITY
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(small.cpu().numpy(), pos[:5].cpu().numpy())
+    st = C.c_uint(0)
+    assert L.HPMCgetDeviceStatus(h, C.byref(st)) == 0 and (st.value & 2)
+    # a bad layout fails lazily like the reference (init.cpp:98-103)
+    L.HPMCsetGridSize(h, 16, 19, 23)
+    assert L.HPMCcreateTraversalHandle(h) is None
+    assert L.HPMCgetLastError(h) == _capi.ERR_LAYOUT
+    L.HPMCdestroyTraversalHandle(th)
+    L.HPMCdestroyHandle(h)
+    L.HPMCunregisterDeviceField(name)
+    L.HPMCdestroyConstants(c)
+
+
+def test_custom_fetch_name_rules(hpmc):
+    from hpmc_b200 import _capi
+
+    L = hpmc.lib()
+    c = L.HPMCcreateConstants(4, 3)
+    h = L.HPMCcreateHistoPyramid(c)
+    L.HPMCsetLatticeSize(h, 16, 16, 16)
+    L.HPMCsetFieldCustom(h, b"float HPMC_fetch(vec3 p) { return p.x; }", 0, 0)
+    assert L.HPMCgetLastError(h) == _capi.ERR_UNSUPPORTED
+    assert L.HPMCgetBuilderProgram(h) == 0  # broken
+    L.HPMCsetFieldCustom(h, b"hpmc:cayley", 0, 0)
+    assert L.HPMCgetBuilderProgram(h) != 0
+    L.HPMCdestroyHandle(h)
+    L.HPMCdestroyConstants(c)
