@@ -27,7 +27,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -61,29 +60,36 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.path = None
 
-    def __enter__(self):
+    def start(self):
+        import tempfile
+
         try:
+            fd, self.path = tempfile.mkstemp(prefix="hpmc_clocks_", suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
+            visible = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            gpu = visible.split(",")[self.gpu] if visible else str(self.gpu)
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+                ["nvidia-smi", f"--id={gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)  # let nvidia-smi start sampling before the GPU work
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def __exit__(self, *exc):
+    def stop(self):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+            self.fh.close()
+            with open(self.path) as f:
+                self.lines = [ln.strip() for ln in f if ln.strip()]
+            os.unlink(self.path)
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -164,7 +170,7 @@ def run_hpmc(args, rank, world, local_rank):
 
     dev = torch.device(f"cuda:{local_rank}")
     torch.cuda.set_device(dev)
-    field_np, iso = datasets.cayley(512)
+    field_np, iso = datasets.cayley(args.lattice)
     fz, fy, fx = field_np.shape
     cells = (fx - 1) * (fy - 1) * (fz - 1)
     field_bytes = field_np.nbytes
@@ -183,10 +189,15 @@ def run_hpmc(args, rank, world, local_rank):
     nrm = torch.empty((nverts, 4), dtype=torch.float32, device=dev)
     th.set_buffers(pos, nrm, nverts)
 
+    path = hp.classify_path()
+
     def step():
         hp.build(iso)
         th.extract()
 
+    # clocks are sampled from the start of the warm-up to the end of the timed
+    # region (a short timed region alone would fall between two samples)
+    clocks = ClockSampler(local_rank).start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
@@ -197,7 +208,7 @@ def run_hpmc(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clocks:
+    if True:
         t_begin = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
         t_begin.record(stream)
@@ -210,6 +221,7 @@ def run_hpmc(args, rank, world, local_rank):
         t_end.record(stream)
         stream.synchronize()
         torch.cuda.synchronize()
+    clocks.stop()
     total_ms = t_begin.elapsed_time(t_end)
     build_ms = [ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps)]
     trav_ms = [ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps)]
@@ -234,7 +246,7 @@ def run_hpmc(args, rank, world, local_rank):
 
     # --- e2e through the public API with host buffers ----------------------
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         h_field = torch.from_numpy(field_np).pin_memory()
         h_pos = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
         h_nrm = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
@@ -274,7 +286,9 @@ def run_hpmc(args, rank, world, local_rank):
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic: seeded Cayley cubic + N(0,1e-3) noise, generated in FP64, stored FP32",
-                "config": {"workload": WORKLOAD, "lattice": [fx, fy, fz], "cells": cells, "vertices": nverts,
+                "config": {"workload": WORKLOAD if args.lattice == 512 else WORKLOAD.replace("512^3", f"{fx}^3"),
+                           "lattice": [fx, fy, fz], "cells": cells, "vertices": nverts,
+                           "classify_path": "tma_column" if path == 1 else "generic",
                            "normals": "central", "l2": "inputs larger than L2 (537 MB field per step)",
                            "parallelism": f"replicas x{world} (independent volumes)"},
                 "roofline": roof,
@@ -297,6 +311,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="hpmc", choices=["hpmc", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--lattice", type=int, default=512, help="lattice edge (profiling runs use smaller ones)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -165,6 +165,12 @@ class HistoPyramid:
         _check(lib().HPMCreadLevel(self.ptr, int(level), out.ctypes.data, n), "HPMCreadLevel")
         return out
 
+    def classify_path(self) -> int:
+        """1: TMA column kernel, 0: generic per-block kernel (last build)."""
+        p = C.c_int(-1)
+        _check(lib().HPMCgetClassifyPath(self.ptr, C.byref(p)), "HPMCgetClassifyPath")
+        return int(p.value)
+
     def device_status(self) -> int:
         s = C.c_uint(0)
         _check(lib().HPMCgetDeviceStatus(self.ptr, C.byref(s)), "HPMCgetDeviceStatus")

@@ -79,6 +79,7 @@ _SIGS = {
     "HPMCreadLevel": (C.c_int, [vp, C.c_int, vp, C.c_size_t]),
     "HPMCsetTraversalDebugBuffers": (C.c_int, [vp, vp, vp]),
     "HPMCgetDeviceStatus": (C.c_int, [vp, C.POINTER(C.c_uint)]),
+    "HPMCgetClassifyPath": (C.c_int, [vp, C.POINTER(C.c_int)]),
 }
 
 _lib = None

@@ -198,7 +198,9 @@ int bind_field(HPMCHistoPyramid* h) {
                                         (cuuint64_t)h->lattice[2]};
             const cuuint64_t strides[2] = {(cuuint64_t)rp, (cuuint64_t)sp};
             const bool f32 = f.type == HPMC_SCALAR_F32;
-            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, 1u};
+            // one ring stage of the column kernel: 32+1 columns padded to a
+            // 16-byte row, 32+1 rows, kLayersPerBox layers
+            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, (cuuint32_t)hpmc::kLayersPerBox};
             const cuuint32_t estr[3] = {1, 1, 1};
             CUresult r = enc(&h->tmap, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
                              const_cast<void*>(f.ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -225,12 +227,21 @@ bool setup(HPMCHistoPyramid* h) {
         V.lattice[i] = h->lattice[i];
         V.cells[i] = h->cells[i];
         V.scale[i] = h->extent[i] / (float)h->cells[i];
+        V.dscale[i] = (double)h->extent[i] / (double)h->cells[i];
     }
     V.tile_x = L[0];
     V.tile_y = L[1];
     V.layout_x = L[2];
     V.layout_y = L[3];
     V.size_l2 = L[4];
+    auto ilog2 = [](int v) {
+        int e = 0;
+        while ((1 << e) < v) e++;
+        return e;
+    };
+    V.wx_l2 = ilog2(2 * L[0]);
+    V.wy_l2 = ilog2(2 * L[1]);
+    V.lx_l2 = ilog2(L[2]);
     V.jtop = std::max(hpmc::kBlockLevel, V.size_l2 + 1);
     // dense levels, top first, each padded to a multiple of 4 entries
     long long off = 0;
@@ -249,6 +260,17 @@ bool setup(HPMCHistoPyramid* h) {
     V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
     V.nfx = (V.cells[0] + 31) / 32;
     V.nfy = (V.cells[1] + 31) / 32;
+    // slices per column CTA: the longest column that still gives ~12 CTAs per SM
+    {
+        const long long target = 12ll * h->constants->num_sms;
+        V.column_slices = hpmc::kColumnSliceChoices[3];
+        for (int zc : hpmc::kColumnSliceChoices) {
+            if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= target) {
+                V.column_slices = zc;
+                break;
+            }
+        }
+    }
     const long long slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
     // (re)allocate
     if ((size_t)levels_total > h->levels_cap || (size_t)slots > h->arena_cap || !h->d_ctrl) {
@@ -467,6 +489,17 @@ void HPMCbuildHistopyramid(HPMCHistoPyramid* h, GLfloat threshold) {
     Volume& V = h->V;
     V.iso = threshold;
     V.binary = h->binary ? 1 : 0;
+    // uint8 fields: f(b) is monotonic in b, so f(b) < iso  <=>  b < u8_thr
+    // (host float division is IEEE, the same rounding as the device's)
+    {
+        const float thr = h->binary ? 0.5f : threshold;
+        int n = 0;
+        for (int b = 0; b < 256; b++) {
+            const float f = (V.ftype == hpmc::kFieldUNorm8) ? (float)b / 255.0f : (float)b;
+            if (f < thr) n = b + 1;
+        }
+        V.u8_thr = n;
+    }
     V.codes_out = h->codes_capture;
     h->threshold = threshold;
     const int max_ctas = h->constants->num_sms * 16;
@@ -723,6 +756,14 @@ int HPMCsetTraversalDebugBuffers(HPMCTraversalHandle* th, int32_t* cell_info, fl
     if (cell_info && (uintptr_t)cell_info % 16) return HPMC_ERR_INVALID_VALUE;
     th->dbg_cell = cell_info;
     th->dbg_t = t;
+    return HPMC_OK;
+}
+
+int HPMCgetClassifyPath(HPMCHistoPyramid* h, int* path) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    if (!path) return HPMC_ERR_INVALID_VALUE;
+    if (!h->built) return HPMC_ERR_NOT_BUILT;
+    *path = (h->V.column_layout && h->have_tmap) ? 1 : 0;
     return HPMC_OK;
 }
 

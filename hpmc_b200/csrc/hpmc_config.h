@@ -11,17 +11,21 @@ constexpr int kFunctorMaxParams = 136;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 
-// Classification: slices per column CTA and TMA ring depth.
-constexpr int kColumnSlices = 32;
-constexpr int kRingStages = 6;
+// Classification: sample layers per TMA box (one ring stage), ring depth, and
+// the slices per column CTA (chosen per volume from kColumnSliceChoices so
+// that slices + 1 layers fill whole boxes and the grid covers the GPU).
+constexpr int kLayersPerBox = 4;
+constexpr int kRingStages = 2;
+constexpr int kColumnSliceChoices[4] = {63, 31, 15, 7};
 
 // Traversal: top pyramid entries cached in shared memory per CTA
 // (levels with <= 1024 entries: 1 + 4 + ... + 1024, each padded to 4).
 constexpr int kTopCacheEntries = 1368;
 // Vertices per warp work item (R rounds of 32).
-constexpr int kTraverseRounds = 4;
+constexpr int kTraverseRounds = 16;
 
-// Bounded waits: iterations of an mbarrier poll before giving up.
-constexpr unsigned int kSpinLimit = 1u << 26;
+// Bounded waits: an mbarrier poll gives up after this long (a TMA box lands
+// in microseconds; only a fault in the copy path gets near it).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
 }  // namespace hpmc

@@ -81,10 +81,14 @@ struct Volume {
     float iso;
     int binary;
     float scale[3];          // extent / cells
-    // layout (init.cpp:72-149)
+    double dscale[3];        // extent / cells in FP64 (geometry)
+    // layout (init.cpp:72-149); all sizes are powers of two
     int tile_x, tile_y;      // texels per tile (cells per tile = 2x)
     int layout_x, layout_y;
     int size_l2;
+    int wx_l2, wy_l2;        // log2 of the cells per tile (2 tile_x, 2 tile_y)
+    int lx_l2;               // log2 of layout_x
+    int u8_thr;              // uint8 fields: sample below iso  <=>  byte < u8_thr
     // compact pyramid
     int jtop;                          // top dense level: max(5, size_l2 + 1)
     uint32_t* levels;                  // dense levels, top level first
@@ -96,6 +100,7 @@ struct Volume {
     // footprints, so only real blocks take memory.  Otherwise slot = block.
     int column_layout;
     int nfx, nfy;                      // 32-cell footprints per slice in x, y
+    int column_slices;                 // slices per column CTA
     uint32_t* arena;                   // kBlockWords words per slot
     long long arena_slots;             // capacity of the arena
     Ctrl* ctrl;
@@ -137,12 +142,11 @@ __host__ __device__ __forceinline__ void morton10(uint32_t m, int& cx, int& cy) 
 // Virtual cell (X, Y) -> lattice cell; false for padding (shadergen.cpp:497-503).
 __host__ __device__ __forceinline__ bool virtual_to_cell(const Volume& V, uint32_t X, uint32_t Y,
                                                          int& x, int& y, int& z) {
-    const uint32_t wx = 2u * (uint32_t)V.tile_x, wy = 2u * (uint32_t)V.tile_y;
-    const uint32_t tu = X / wx, tv = Y / wy;
-    x = (int)(X - tu * wx);
-    y = (int)(Y - tv * wy);
+    const uint32_t tu = X >> V.wx_l2, tv = Y >> V.wy_l2;
+    x = (int)(X & ((1u << V.wx_l2) - 1u));
+    y = (int)(Y & ((1u << V.wy_l2) - 1u));
     if (tu >= (uint32_t)V.layout_x || tv >= (uint32_t)V.layout_y) return false;
-    z = (int)(tv * (uint32_t)V.layout_x + tu);
+    z = (int)((tv << V.lx_l2) | tu);
     return x < V.cells[0] && y < V.cells[1] && z < V.cells[2];
 }
 
@@ -171,9 +175,9 @@ __host__ __device__ __forceinline__ long long block_slot(const Volume& V, uint64
 
 // Block index of footprint (fx, fy) of slice z (column layout).
 __host__ __device__ __forceinline__ uint64_t column_block_index(const Volume& V, int z, int fx, int fy) {
-    const uint32_t tu = (uint32_t)z % (uint32_t)V.layout_x, tv = (uint32_t)z / (uint32_t)V.layout_x;
-    const uint32_t X0 = 2u * (uint32_t)V.tile_x * tu + 32u * (uint32_t)fx;
-    const uint32_t Y0 = 2u * (uint32_t)V.tile_y * tv + 32u * (uint32_t)fy;
+    const uint32_t tu = (uint32_t)z & ((1u << V.lx_l2) - 1u), tv = (uint32_t)z >> V.lx_l2;
+    const uint32_t X0 = (tu << V.wx_l2) + 32u * (uint32_t)fx;
+    const uint32_t Y0 = (tv << V.wy_l2) + 32u * (uint32_t)fy;
     return morton_spread(X0 >> 5) | (morton_spread(Y0 >> 5) << 1);
 }
 

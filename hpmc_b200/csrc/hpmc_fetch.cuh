@@ -84,14 +84,28 @@ __device__ __forceinline__ void functor_gradient(const FunctorParams& F, float p
     }
 }
 
+// uint8 -> float without the conversion pipe: exact for b < 2^23.
+__device__ __forceinline__ float u8_to_float(uint32_t b) {
+    return __int_as_float(0x4B000000u | b) - 8388608.0f;
+}
+
+// b/255 correctly rounded (GL's UNORM8 -> float) with two FMAs; equal to the
+// IEEE quotient for every b in 0..255 (checked exhaustively).
+__device__ __forceinline__ float unorm8_to_float(uint32_t b) {
+    const float fb = u8_to_float(b);
+    const float r255 = 1.0f / 255.0f;
+    const float q = fb * r255;
+    return fmaf(fmaf(-q, 255.0f, fb), r255, q);
+}
+
 template <int FT>
 __device__ __forceinline__ float fetch_raw(const Volume& V, long long off) {
     if constexpr (FT == kFieldF32) {
         return __ldg(static_cast<const float*>(V.field) + off);
     } else if constexpr (FT == kFieldU8) {
-        return (float)__ldg(static_cast<const unsigned char*>(V.field) + off);
+        return u8_to_float(__ldg(static_cast<const unsigned char*>(V.field) + off));
     } else {
-        return __fdiv_rn((float)__ldg(static_cast<const unsigned char*>(V.field) + off), 255.0f);
+        return unorm8_to_float(__ldg(static_cast<const unsigned char*>(V.field) + off));
     }
 }
 

@@ -39,12 +39,37 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false if the phase did not complete within `limit` polls.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
+// try_wait that lets the hardware suspend the thread for up to `hint_ns`
+// while the phase is incomplete (no spinning on the issue slots).
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false if the phase did not complete within `limit_ns`
+// nanoseconds or once another CTA has raised `abort_bits` in *status.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns,
+                                                  const unsigned int* status, unsigned int abort_bits) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait_suspend(bar, parity, 20000u)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+        if (status && (*(volatile const unsigned int*)status & abort_bits)) return false;
     }
-    return false;
 }
 
 // 3-D tiled TMA load of one box into this CTA's shared memory; x must be

@@ -63,18 +63,141 @@ __device__ __forceinline__ void write_codes(const Volume& V, uint32_t packed, in
 
 // ---------------------------------------------------------------------------
 // Column classification: CTA = one 32x32 cell footprint of the slice tiles,
-// streaming kColumnSlices slices through a TMA ring of sample layers.  Each
-// sample is fetched from HBM once (layer halo rows/columns are shared with
-// the neighbouring CTAs through L2).  Layer values become one bit per sample
-// (f < iso) in shared memory; every thread then forms the codes of one 2x2
-// quad of cells, counts them and the CTA sums 1024 cells into one level-5
-// entry.  Non-empty blocks store their codes in the arena.
+// streaming column_slices slices through a TMA ring of 4-layer sample boxes (each
+// sample leaves HBM once; halo rows/columns are shared with neighbouring
+// CTAs through L2).
+//
+// Per layer, every warp turns rows of samples into bits (f < iso) with one
+// ballot per row.  Per slice, ONE warp classifies the whole 32x32 block,
+// bit-sliced: lane y holds the 32 cells of row y as eight 32-bit words, word
+// k = bit k (dx + 2dy + 4dz) of the 32 codes.  AND/OR over the eight words
+// marks the cells that are neither all-inside nor all-outside (the only ones
+// with vertices); only those go through the count table.  The warp sum is the
+// block's level-5 entry; non-empty blocks also store their 1024 codes
+// (bit-matrix transpose) in the arena.
+namespace {
+
+template <int FT, typename T>
+__device__ __forceinline__ bool below(T v, float iso, int u8_thr) {
+    if constexpr (FT == kFieldF32)
+        return v < iso;  // strict; NaN -> false (shadergen.cpp:137-142)
+    else
+        return (int)v < u8_thr;
+}
+
+// 8x8 bit-matrix transpose: byte r bit c -> byte c bit r.
+__device__ __forceinline__ uint64_t transpose8(uint64_t x) {
+    uint64_t t;
+    t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+    x = x ^ t ^ (t << 7);
+    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+    x = x ^ t ^ (t << 14);
+    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+    x = x ^ t ^ (t << 28);
+    return x;
+}
+
+// Bit-sliced codes of one 32-cell row -> 32 byte codes (w[i] = cells 4i..4i+3).
+__device__ __forceinline__ void slices_to_codes(const uint32_t c[8], uint32_t w[8]) {
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+        const uint32_t sel = (uint32_t)g | ((uint32_t)(g + 4) << 4);
+        const uint32_t lo = __byte_perm(__byte_perm(c[0], c[1], sel), __byte_perm(c[2], c[3], sel), 0x5410);
+        const uint32_t hi = __byte_perm(__byte_perm(c[4], c[5], sel), __byte_perm(c[6], c[7], sel), 0x5410);
+        const uint64_t x = transpose8((uint64_t)lo | ((uint64_t)hi << 32));
+        w[2 * g] = (uint32_t)x;
+        w[2 * g + 1] = (uint32_t)(x >> 32);
+    }
+}
+
+// One warp: classify slice z of footprint (fx, fy) from sample-bit rows of the
+// lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).
+__device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, int lane,
+                                                    uint32_t vmask, const uint32_t* rows_b, uint64_t col_b,
+                                                    const uint32_t* rows_t, uint64_t col_t,
+                                                    const uint8_t* s_cnt) {
+    // 33-bit rows y and y+1 of both layers (bit 32 = column x0+32)
+    const uint64_t A0 = rows_b[lane] | (((col_b >> lane) & 1ull) << 32);
+    const uint64_t A1 = rows_b[lane + 1] | (((col_b >> (lane + 1)) & 1ull) << 32);
+    const uint64_t B0 = rows_t[lane] | (((col_t >> lane) & 1ull) << 32);
+    const uint64_t B1 = rows_t[lane + 1] | (((col_t >> (lane + 1)) & 1ull) << 32);
+    uint32_t c[8];
+    c[0] = (uint32_t)A0;         // (x,   y,   z)
+    c[1] = (uint32_t)(A0 >> 1);  // (x+1, y,   z)
+    c[2] = (uint32_t)A1;         // (x,   y+1, z)
+    c[3] = (uint32_t)(A1 >> 1);
+    c[4] = (uint32_t)B0;         // (x,   y,   z+1)
+    c[5] = (uint32_t)(B0 >> 1);
+    c[6] = (uint32_t)B1;
+    c[7] = (uint32_t)(B1 >> 1);
+    uint32_t all = c[0], any = c[0];
+#pragma unroll
+    for (int k = 1; k < 8; k++) {
+        all &= c[k];
+        any |= c[k];
+    }
+    uint32_t active = (all ^ any) & vmask;
+    uint32_t cnt = 0;
+    while (active) {
+        const int x = __ffs(active) - 1;
+        uint32_t code = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) code |= ((c[k] >> x) & 1u) << k;
+        cnt += s_cnt[code];
+        active &= active - 1;
+    }
+    const uint32_t total = __reduce_add_sync(0xffffffffu, cnt);
+    const uint64_t b = column_block_index(V, z, fx, fy);
+    if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
+    if (total == 0 && !V.codes_out) return;
+    // codes of this row (cells outside the grid are masked to 0)
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] &= vmask;
+    uint32_t w[8];
+    slices_to_codes(c, w);
+    if (total) {
+        // arena word for quad (qx, qy) = cells (2qx,2qy),(2qx+1,2qy),(2qx,2qy+1),(2qx+1,2qy+1):
+        // rows 2qy (even lane) and 2qy+1 (odd lane); even lanes store qx 0..7, odd 8..15
+        uint32_t p[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) p[i] = __shfl_xor_sync(0xffffffffu, w[i], 1);
+        const bool odd = lane & 1;
+        const uint32_t qy = (uint32_t)lane >> 1;
+        const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
+        uint32_t* dst = V.arena + slot * kBlockWords;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t qx = (odd ? 8u : 0u) + (uint32_t)i;
+            const uint32_t wi = odd ? w[4 + (i >> 1)] : w[i >> 1];  // this lane's word with cells 2qx, 2qx+1
+            const uint32_t pi = odd ? p[4 + (i >> 1)] : p[i >> 1];
+            const uint32_t upper = odd ? wi : pi;  // row 2qy+1
+            const uint32_t lower = odd ? pi : wi;  // row 2qy
+            const uint32_t word = __byte_perm(lower, upper, (i & 1) ? 0x7632 : 0x5410);
+            const uint32_t q = (uint32_t)(morton_spread(qx) | (morton_spread(qy) << 1));
+            dst[q] = word;
+        }
+    }
+    if (V.codes_out) {
+        const int y = fy * 32 + lane;
+        if (y < V.cells[1]) {
+            uint8_t* row = V.codes_out + ((long long)z * V.cells[1] + y) * V.cells[0] + fx * 32;
+            const int nx = min(32, V.cells[0] - fx * 32);
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                if (i < nx) row[i] = (uint8_t)(w[i >> 2] >> (8 * (i & 3)));
+        }
+    }
+}
+
+}  // namespace
+
 template <int FT>
 __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_constant__ CUtensorMap tmap,
                                                                 const __grid_constant__ Volume V) {
     using T = typename std::conditional<FT == kFieldF32, float, uint8_t>::type;
-    constexpr int BXE = (FT == kFieldF32) ? 36 : 48;       // box width (16-byte multiple)
-    constexpr int STAGE_BYTES = BXE * 33 * (int)sizeof(T);  // one sample layer
+    constexpr int BXE = (FT == kFieldF32) ? 36 : 48;  // box width (16-byte multiple)
+    constexpr int LAYER = BXE * 33;                    // elements of one sample layer
+    constexpr int STAGE_BYTES = LAYER * kLayersPerBox * (int)sizeof(T);
     constexpr int STAGE_STRIDE = (STAGE_BYTES + 127) & ~127;
 
     extern __shared__ __align__(128) uint8_t s_dyn[];
@@ -82,17 +205,19 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     // (the launch reserves 128 spare bytes)
     uint8_t* const s_ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
     __shared__ __align__(8) uint64_t s_bar[kRingStages];
-    __shared__ uint64_t s_rows[3][33];
-    __shared__ uint32_t s_warp[2][kWarps];
+    __shared__ __align__(16) uint32_t s_rows[8][36];  // layer % 8: bit x = sample (x0 + x, y0 + r) below iso
+    __shared__ uint64_t s_col[8];       // layer % 8: bit r = sample (x0 + 32, y0 + r) below iso
     __shared__ uint8_t s_cnt[256];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int fx = blockIdx.x, fy = blockIdx.y;
     const int x0 = fx * 32, y0 = fy * 32;
-    const int z0 = blockIdx.z * kColumnSlices;
-    const int z1 = min(V.cells[2], z0 + kColumnSlices);
+    const int z0 = blockIdx.z * V.column_slices;
+    const int z1 = min(V.cells[2], z0 + V.column_slices);
     const int nlayers = z1 - z0 + 1;
+    const int nbox = (nlayers + kLayersPerBox - 1) / kLayersPerBox;
     const float iso = V.binary ? 0.5f : V.iso;
+    const int u8_thr = V.u8_thr;
 
     s_cnt[tid] = c_vertex_count[tid];
     if (tid == 0) {
@@ -101,98 +226,73 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     }
     __syncthreads();
     if (tid == 0) {
-        for (int s = 0; s < kRingStages && s < nlayers; s++) {
-            mbar_arrive_expect_tx(&s_bar[s], STAGE_BYTES);
-            tma_load_3d(s_ring + s * STAGE_STRIDE, &tmap, x0, y0, z0 + s, &s_bar[s]);
+        for (int k = 0; k < kRingStages && k < nbox; k++) {
+            mbar_arrive_expect_tx(&s_bar[k], STAGE_BYTES);
+            tma_load_3d(s_ring + k * STAGE_STRIDE, &tmap, x0, y0, z0 + k * kLayersPerBox, &s_bar[k]);
         }
     }
+    // cells of this lane's row inside the grid (masked codes are 0, shadergen.cpp:112-125)
+    const int xv = V.cells[0] - x0;
+    const uint32_t xmask = xv >= 32 ? 0xffffffffu : ((1u << xv) - 1u);
+    const uint32_t vmask = (y0 + lane < V.cells[1]) ? xmask : 0u;
 
-    // this thread's quad (Morton order inside the 16x16 quads of the block)
-    int qx, qy;
-    morton10((uint32_t)tid, qx, qy);
-    const int cx0 = x0 + 2 * qx, cy0 = y0 + 2 * qy;
-    const bool vx0 = cx0 < V.cells[0], vx1 = cx0 + 1 < V.cells[0];
-    const bool vy0 = cy0 < V.cells[1], vy1 = cy0 + 1 < V.cells[1];
-
-    uint32_t packed_prev = 0;
     bool timed_out = false;
-    int li = 0;
-    for (; li < nlayers; li++) {
-        const int s = li % kRingStages;
-        const uint32_t parity = (uint32_t)(li / kRingStages) & 1u;
-        if (!mbar_wait_bounded(&s_bar[s], parity, kSpinLimit)) timed_out = true;
-        if (!timed_out) {
-            // layer li -> one bit per sample, rows of 33 bits
-            const T* st = reinterpret_cast<const T*>(s_ring + s * STAGE_STRIDE);
-            for (int r = warp; r < 33; r += kWarps) {
-                const float v = (float)st[r * BXE + lane];
-                const float v32 = (float)st[r * BXE + 32];
-                float vv = v, vv32 = v32;
-                if (FT == kFieldUNorm8) {
-                    vv = __fdiv_rn(v, 255.0f);
-                    vv32 = __fdiv_rn(v32, 255.0f);
+    int k = 0;
+    for (; k < nbox; k++) {
+        const int s = k % kRingStages;
+        const uint32_t parity = (uint32_t)(k / kRingStages) & 1u;
+        // one warp polls the box's barrier; the others wait at the CTA barrier
+        if (warp == 0 && !mbar_wait_bounded(&s_bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout))
+            timed_out = true;
+        if (__syncthreads_or(timed_out)) break;
+        if (warp != 0) mbar_try_wait(&s_bar[s], parity);  // completed phase: acquire the TMA writes
+        const int lb = k * kLayersPerBox;
+        const int nl = min(kLayersPerBox, nlayers - lb);
+        const T* st = reinterpret_cast<const T*>(s_ring + s * STAGE_STRIDE);
+#pragma unroll
+        for (int l = 0; l < kLayersPerBox; l++) {
+            if (l < nl) {
+                // warp w: rows 4w .. 4w+3 (one ballot per row, one 16-byte store)
+                const T* layer = st + l * LAYER;
+                const int buf = (lb + l) & 7;
+                const T* row = layer + 4 * warp * BXE + lane;
+                const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(row[0], iso, u8_thr));
+                const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(row[BXE], iso, u8_thr));
+                const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(row[2 * BXE], iso, u8_thr));
+                const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(row[3 * BXE], iso, u8_thr));
+                if (lane == 0) *reinterpret_cast<uint4*>(&s_rows[buf][4 * warp]) = make_uint4(b0, b1, b2, b3);
+                if (warp == kWarps - 1 - l) {  // row 32 and column x0+32
+                    const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(layer[32 * BXE + lane], iso, u8_thr));
+                    const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(layer[lane * BXE + 32], iso, u8_thr));
+                    const bool corner = below<FT>(layer[32 * BXE + 32], iso, u8_thr);
+                    if (lane == 0) {
+                        s_rows[buf][32] = r32;
+                        s_col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
+                    }
                 }
-                const uint32_t b = __ballot_sync(0xffffffffu, vv < iso);
-                if (lane == 0) s_rows[li % 3][r] = (uint64_t)b | ((uint64_t)(vv32 < iso) << 32);
             }
         }
-        if (__syncthreads_or(timed_out)) break;  // barrier A: stage s is free, rows li ready
-        if (tid == 0 && li + kRingStages < nlayers) {
+        __syncthreads();  // stage s consumed; bit rows of layers lb .. lb+nl-1 ready
+        if (tid == 0 && k + kRingStages < nbox) {
             mbar_arrive_expect_tx(&s_bar[s], STAGE_BYTES);
-            tma_load_3d(s_ring + s * STAGE_STRIDE, &tmap, x0, y0, z0 + li + kRingStages, &s_bar[s]);
+            tma_load_3d(s_ring + s * STAGE_STRIDE, &tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox, &s_bar[s]);
         }
-        // finalise slice li-2 (its warp sums were published before this barrier)
-        if (li >= 2) {
-            const int z = z0 + li - 2;
-            uint32_t total = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; w++) total += s_warp[(li - 2) & 1][w];
-            const uint64_t b = column_block_index(V, z, fx, fy);
-            if (tid == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-            if (total) {
-                const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
-                V.arena[slot * kBlockWords + tid] = packed_prev;
-            }
-            if (V.codes_out) write_codes(V, packed_prev, cx0, cy0, z);
-        }
-        // classify slice li-1 from sample layers li-1 (bottom) and li (top)
-        if (li >= 1) {
-            const uint64_t* rb = s_rows[(li - 1) % 3];
-            const uint64_t* rt = s_rows[li % 3];
-            uint32_t gb[3], gt[3];
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                gb[j] = (uint32_t)(rb[2 * qy + j] >> (2 * qx)) & 7u;
-                gt[j] = (uint32_t)(rt[2 * qy + j] >> (2 * qx)) & 7u;
-            }
-            const uint32_t packed = quad_codes(gb, gt, vx0, vx1, vy0, vy1);
-            const uint32_t cnt = __reduce_add_sync(0xffffffffu, quad_count(s_cnt, packed));
-            if (lane == 0) s_warp[(li - 1) & 1][warp] = cnt;
-            packed_prev = packed;
+        // slices whose upper layer arrived in this box, one warp each; row
+        // buffers of a layer stay untouched until two boxes later
+        const int sl = lb - 1 + warp;  // slice (local) = its lower layer
+        if (warp < nl && sl >= 0) {
+            const int bb = sl & 7, bt = (sl + 1) & 7;
+            classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, s_rows[bb], s_col[bb], s_rows[bt], s_col[bt],
+                                s_cnt);
         }
     }
     if (timed_out) {
-        // drain the loads still in flight (bounded) before the CTA exits
+        // drain the boxes still in flight (bounded) before the CTA exits
         if (tid == 0) {
-            for (int l = li; l < nlayers && l < li + kRingStages; l++)
-                mbar_wait_bounded(&s_bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, kSpinLimit);
+            for (int l = k; l < nbox && l < k + kRingStages; l++)
+                mbar_wait_bounded(&s_bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, kWaitLimitNs, nullptr, 0u);
             atomicOr(&V.ctrl->status, kStatusTimeout);
         }
-        return;
-    }
-    __syncthreads();
-    if (nlayers >= 2) {  // finalise the last slice
-        const int z = z0 + nlayers - 2;
-        uint32_t total = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; w++) total += s_warp[(nlayers - 2) & 1][w];
-        const uint64_t b = column_block_index(V, z, fx, fy);
-        if (tid == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-        if (total) {
-            const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
-            V.arena[slot * kBlockWords + tid] = packed_prev;
-        }
-        if (V.codes_out) write_codes(V, packed_prev, cx0, cy0, z);
     }
 }
 
@@ -211,12 +311,11 @@ __device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b,
     const uint32_t Y = (morton_compact(b >> 1) << 5) + 2u * (uint32_t)qy;
     int x = 0, y = 0, z = 0;
     uint32_t packed = 0;
-    const uint32_t wx = 2u * (uint32_t)V.tile_x, wy = 2u * (uint32_t)V.tile_y;
-    const uint32_t tu = X / wx, tv = Y / wy;
+    const uint32_t tu = X >> V.wx_l2, tv = Y >> V.wy_l2;
     if (tu < (uint32_t)V.layout_x && tv < (uint32_t)V.layout_y) {
-        x = (int)(X - tu * wx);
-        y = (int)(Y - tv * wy);
-        z = (int)(tv * (uint32_t)V.layout_x + tu);
+        x = (int)(X & ((1u << V.wx_l2) - 1u));
+        y = (int)(Y & ((1u << V.wy_l2) - 1u));
+        z = (int)((tv << V.lx_l2) | tu);
         if (z < V.cells[2] && x < V.cells[0] && y < V.cells[1]) {
             uint32_t gb[3], gt[3];
 #pragma unroll
@@ -260,7 +359,8 @@ __global__ void __launch_bounds__(kThreads) classify_blocks(const __grid_constan
 // of level j_in in shared memory (6 levels); the last CTA to finish carries
 // on from those partial tops to level j_stop.  The top entry is the vertex
 // count (hpiface.cpp:323-327).
-constexpr int kReduceChunk = 4096;
+constexpr int kReduceChunk = 1024;  // level entries per CTA (5 levels)
+constexpr int kReduceTop = 4096;    // entries the last CTA can finish (6 levels)
 
 __device__ __forceinline__ bool level5_valid(const Volume& V, uint64_t b) {
     int z, fx, fy;
@@ -270,7 +370,7 @@ __device__ __forceinline__ bool level5_valid(const Volume& V, uint64_t b) {
 __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int& j, int j_stop, long long n,
                             long long out_base, bool& overflow) {
     // buf0 holds n entries of level j (n a power of 4); out_base = index of the
-    // first entry of level j in this chunk.
+    // first entry of level j in this chunk.  Leaves the last level in buf0.
     uint32_t* src = buf0;
     uint32_t* dst = buf1;
     while (j < j_stop && n >= 4) {
@@ -278,7 +378,8 @@ __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int
         out_base >>= 2;
         j++;
         for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-            const unsigned long long s = (unsigned long long)src[4 * i] + src[4 * i + 1] + src[4 * i + 2] + src[4 * i + 3];
+            const unsigned long long s =
+                (unsigned long long)src[4 * i] + src[4 * i + 1] + src[4 * i + 2] + src[4 * i + 3];
             if (s > 0xffffffffull) overflow = true;
             dst[i] = (uint32_t)s;
             V.levels[V.level_off[j] + out_base + i] = (uint32_t)s;
@@ -288,7 +389,7 @@ __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int
         src = dst;
         dst = t;
     }
-    if (src != buf0) {  // leave the result in buf0
+    if (src != buf0) {
         for (long long i = threadIdx.x; i < n; i += blockDim.x) buf0[i] = src[i];
         __syncthreads();
     }
@@ -296,23 +397,30 @@ __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int
 
 __global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant__ Volume V, int j_in, int j_stop,
                                                           int mask_level5) {
-    __shared__ uint32_t buf0[kReduceChunk];
-    __shared__ uint32_t buf1[kReduceChunk / 4];
+    __shared__ __align__(16) uint32_t buf0[kReduceTop];
+    __shared__ uint32_t buf1[kReduceTop / 4];
     __shared__ int s_last;
     bool overflow = false;
     const long long n_in = level_entries(V.size_l2, j_in);
     const long long base = (long long)blockIdx.x * kReduceChunk;
-    const long long n = min((long long)kReduceChunk, n_in - base);
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-        uint32_t v = V.levels[V.level_off[j_in] + base + i];
-        if (mask_level5 && !level5_valid(V, (uint64_t)(base + i))) v = 0;
-        buf0[i] = v;
+    const long long n = min((long long)kReduceChunk, n_in - base);  // a power of 4 (>= 4)
+    const int t = threadIdx.x;
+    if (4 * t < n) {
+        uint4 v = *reinterpret_cast<const uint4*>(V.levels + V.level_off[j_in] + base + 4 * t);
+        if (mask_level5) {  // level-5 entries of padding blocks are never written
+            const uint64_t e = (uint64_t)(base + 4 * t);
+            if (!level5_valid(V, e)) v.x = 0;
+            if (!level5_valid(V, e + 1)) v.y = 0;
+            if (!level5_valid(V, e + 2)) v.z = 0;
+            if (!level5_valid(V, e + 3)) v.w = 0;
+        }
+        *reinterpret_cast<uint4*>(&buf0[4 * t]) = v;
     }
     __syncthreads();
     int j = j_in;
     reduce_tree(V, buf0, buf1, j, j_stop, n, base, overflow);
     if (j < j_stop) {
-        // more levels remain above this chunk's top: last CTA continues
+        // levels remain above this chunk's top: the last CTA to finish continues
         __threadfence();
         if (threadIdx.x == 0) s_last = (atomicAdd(&V.ctrl->reduce_done, 1u) == gridDim.x - 1);
         __syncthreads();
@@ -321,9 +429,8 @@ __global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant_
             return;
         }
         __threadfence();
-        const long long m = level_entries(V.size_l2, j);  // == gridDim.x entries
-        for (long long i = threadIdx.x; i < m; i += blockDim.x)
-            buf0[i] = __ldcg(&V.levels[V.level_off[j] + i]);
+        const long long m = level_entries(V.size_l2, j);  // == gridDim.x entries, <= kReduceTop
+        for (long long i = threadIdx.x; i < m; i += blockDim.x) buf0[i] = __ldcg(&V.levels[V.level_off[j] + i]);
         __syncthreads();
         reduce_tree(V, buf0, buf1, j, j_stop, m, 0, overflow);
         if (threadIdx.x == 0) V.ctrl->reduce_done = 0;
@@ -339,12 +446,12 @@ __global__ void copy_total(const __grid_constant__ Volume V) {
 
 // ---------------------------------------------------------------------------
 // Host launchers
-constexpr int kRingBytesF32 = kRingStages * ((36 * 33 * 4 + 127) & ~127) + 128;
-constexpr int kRingBytesU8 = kRingStages * ((48 * 33 + 127) & ~127) + 128;
+constexpr int kRingBytesF32 = kRingStages * ((36 * 33 * 4 * kLayersPerBox + 127) & ~127) + 128;
+constexpr int kRingBytesU8 = kRingStages * ((48 * 33 * kLayersPerBox + 127) & ~127) + 128;
 
 cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ctas, cudaStream_t st) {
     if (V.column_layout && tmap) {
-        const int nz = (V.cells[2] + kColumnSlices - 1) / kColumnSlices;
+        const int nz = (V.cells[2] + V.column_slices - 1) / V.column_slices;
         const dim3 grid(V.nfx, V.nfy, nz);
         if (V.ftype == kFieldF32)
             classify_column_tma<kFieldF32><<<grid, kThreads, kRingBytesF32, st>>>(*tmap, V);
@@ -372,8 +479,8 @@ cudaError_t launch_reduce(const Volume& V, cudaStream_t st) {
     }
     int j_in = kBlockLevel;
     while (j_in < V.jtop) {
-        // one launch reduces 6 levels per CTA plus up to 6 more in the last CTA
-        const int j_stop = (V.jtop - j_in <= 12) ? V.jtop : j_in + 6;
+        // one launch reduces 5 levels per CTA plus up to 6 more in the last CTA
+        const int j_stop = (V.jtop - j_in <= 11) ? V.jtop : j_in + 5;
         const long long n_in = level_entries(V.size_l2, j_in);
         const long long grid = (n_in + kReduceChunk - 1) / kReduceChunk;
         reduce_levels<<<(unsigned)grid, kThreads, 0, st>>>(V, j_in, j_stop,

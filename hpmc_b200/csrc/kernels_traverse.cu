@@ -7,22 +7,25 @@
 //
 // Here one persistent grid walks the vertex range; a warp owns 32 consecutive
 // vertices per round:
-//   1. descent: each lane descends the dense levels from the top (cached in
-//      shared memory) to its 1024-key block, choosing the first child whose
-//      running sum exceeds the key exactly as shadergen.cpp:448-467 does; lanes
-//      of a warp read the same entries, so the loads broadcast.  A warp keeps
-//      its current block and skips the descent for vertices inside it.
+//   1. descent (warp-cooperative): the warp descends the dense levels for the
+//      first vertex not covered by its cached block, from the top (cached in
+//      shared memory) to the 1024-key block, taking the first child whose
+//      running sum exceeds the key exactly as shadergen.cpp:448-467 does.  All
+//      lanes walk the same path, so every load is one broadcast transaction;
+//      consecutive vertices reuse the block and skip the descent.
 //   2. in-block lookup (warp-cooperative): the warp loads the block's 1024
-//      codes from the arena, each lane turns 32 of them into vertex counts,
-//      a warp scan gives the block's per-cell prefix sums in shared memory,
-//      and each lane binary-searches its key (shadergen.cpp:469-495).
+//      codes from the arena, each lane turns 32 of them into vertex counts, a
+//      warp scan gives the block's per-cell prefix sums in shared memory, and
+//      each lane binary-searches its key (shadergen.cpp:469-495).
 //   3. geometry (shadergen.cpp:497-563): edge from the case table, crossing
-//      parameter t, position and normal in FP32; coalesced float4 stores.
+//      parameter t, position and normal; FP32 samples and outputs with FP64
+//      intermediates; coalesced streaming float4 stores.
 #include <cuda_runtime.h>
 #include <cstdint>
 
 #include "hpmc_device.cuh"
 #include "hpmc_fetch.cuh"
+#include "hpmc_geometry.cuh"
 #include "hpmc_kernels.h"
 #include "_gen/hpmc_case_tables.h"
 
@@ -33,7 +36,7 @@ __constant__ uint64_t c_edge_nibbles[256] = HPMC_GEN_EDGE_NIBBLES;
 __device__ const float g_binary_normals[256 * 16 * 3] = HPMC_GEN_BINARY_NORMALS;
 constexpr uint64_t kEdgeGeometry = HPMC_GEN_EDGE_GEOMETRY;
 
-enum { kModeForward = 0, kModeCentral = 1, kModeBinary = 2 };
+enum { kModeForward = kGeomForward, kModeCentral = kGeomCentral, kModeBinary = kGeomBinary };
 
 namespace {
 
@@ -54,65 +57,52 @@ __device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
     __syncthreads();
 }
 
-// Descent through the dense levels (jtop-1 .. 5) for vertex key v.
-__device__ __forceinline__ void descend(const Volume& V, const TraverseSmem& S, unsigned long long v,
-                                        unsigned long long& block, unsigned long long& base,
-                                        unsigned int& count) {
-    unsigned long long node = 0, key = v;
+// Descent through the dense levels (jtop-1 .. 5) for vertex key `key`
+// (warp-uniform: every lane passes the same key).
+__device__ __forceinline__ void descend(const Volume& V, const TraverseSmem& S, uint32_t key, uint32_t& block,
+                                        uint32_t& base, uint32_t& count) {
+    uint32_t node = 0;
     base = 0;
-    count = V.levels[V.level_off[V.jtop]];
+    count = V.top_cached ? S.top[0] : V.levels[V.level_off[V.jtop]];
     for (int j = V.jtop - 1; j >= kBlockLevel; j--) {
-        const long long idx = V.level_off[j] + 4ll * (long long)node;
-        uint4 s;
-        if (idx + 4 <= V.top_cached)
-            s = *reinterpret_cast<const uint4*>(&S.top[idx]);
-        else
-            s = __ldg(reinterpret_cast<const uint4*>(V.levels + idx));
-        const unsigned long long s0 = s.x, s1 = s0 + s.y, s2 = s1 + s.z;
-        unsigned long long skip;
-        unsigned int c, cnt;
-        if (key < s0) {
-            c = 0; skip = 0; cnt = s.x;
-        } else if (key < s1) {
-            c = 1; skip = s0; cnt = s.y;
-        } else if (key < s2) {
-            c = 2; skip = s1; cnt = s.z;
-        } else {
-            c = 3; skip = s2; cnt = s.w;
-        }
+        const uint32_t idx = (uint32_t)V.level_off[j] + 4u * node;
+        const uint4 s = (idx + 4u <= (uint32_t)V.top_cached)
+                            ? *reinterpret_cast<const uint4*>(&S.top[idx])
+                            : __ldg(reinterpret_cast<const uint4*>(V.levels + idx));
+        const uint32_t s0 = s.x, s1 = s0 + s.y, s2 = s1 + s.z;
+        const uint32_t c = (uint32_t)(key >= s0) + (uint32_t)(key >= s1) + (uint32_t)(key >= s2);
+        const uint32_t skip = c == 0 ? 0u : c == 1 ? s0 : c == 2 ? s1 : s2;
+        count = c == 0 ? s.x : c == 1 ? s.y : c == 2 ? s.z : s.w;
         key -= skip;
         base += skip;
-        node = 4ull * node + c;
-        count = cnt;
+        node = 4u * node + c;
     }
     block = node;
 }
 
 // Warp-cooperative: per-cell inclusive prefix of vertex counts of block b.
-__device__ __forceinline__ void load_block(const Volume& V, TraverseSmem& S, int warp, int lane,
-                                           unsigned long long b) {
+__device__ __forceinline__ void load_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t b) {
     const long long slot = block_slot(V, b);
     const uint4* src = reinterpret_cast<const uint4*>(V.arena + slot * kBlockWords) + 2 * lane;
     const uint4 w0 = __ldg(src), w1 = __ldg(src + 1);
     const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
     uint32_t run = 0;
-    uint32_t incl[32];
 #pragma unroll
-    for (int i = 0; i < 32; i++) {
-        run += S.cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
-        incl[i] = run;
-    }
-    // exclusive scan of the lane sums
-    uint32_t scan = run;
+    for (int i = 0; i < 32; i++) run += S.cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+    uint32_t scan = run;  // inclusive scan of the lane sums
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
         if (lane >= o) scan += t;
     }
-    const uint32_t excl = scan - run;
+    uint32_t acc = scan - run;
     uint32_t* pref32 = reinterpret_cast<uint32_t*>(&S.pref[warp][32 * lane]);
 #pragma unroll
-    for (int i = 0; i < 16; i++) pref32[i] = (excl + incl[2 * i]) | ((excl + incl[2 * i + 1]) << 16);
+    for (int i = 0; i < 16; i++) {
+        const uint32_t a = acc + S.cnt[(w[i >> 1] >> (16 * (i & 1))) & 0xffu];
+        acc = a + S.cnt[(w[i >> 1] >> (16 * (i & 1) + 8)) & 0xffu];
+        pref32[i] = a | (acc << 16);
+    }
     uint4* cw = reinterpret_cast<uint4*>(&S.codew[warp][8 * lane]);
     cw[0] = w0;
     cw[1] = w1;
@@ -126,8 +116,8 @@ struct VertexCell {
     int k;
 };
 
-__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp,
-                                                unsigned long long b, unsigned int key) {
+__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp, uint32_t b,
+                                                uint32_t key) {
     const uint16_t* pref = S.pref[warp];
     int lo = 0;
 #pragma unroll
@@ -140,33 +130,27 @@ __device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseS
     int cx, cy;
     morton10((uint32_t)lo, cx, cy);
     const uint32_t X = (morton_compact(b) << 5) + (uint32_t)cx;
-    const uint32_t Y = (morton_compact(b >> 1) << 5) + (uint32_t)cy;
+    const uint32_t Y = (morton_compact((uint64_t)b >> 1) << 5) + (uint32_t)cy;
     virtual_to_cell(V, X, Y, r.x, r.y, r.z);
     return r;
 }
 
 // Steps 1-2 for one round of 32 vertices of a warp; returns false for lanes
 // without a vertex.  (bb, bbase, bcount) is the warp's cached block.
-__device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S, int warp, int lane,
-                                               unsigned long long v, bool act, long long& bb,
-                                               unsigned long long& bbase, unsigned int& bcount,
-                                               VertexCell& out) {
-    unsigned long long myb = (unsigned long long)bb, mybase = bbase;
-    unsigned int mycnt = bcount;
-    const bool cached = bb >= 0 && v >= bbase && v < bbase + bcount;
-    if (act && !cached) descend(V, S, v, myb, mybase, mycnt);
+__device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t v,
+                                               bool act, uint32_t& bb, uint32_t& bbase, uint32_t& bcount,
+                                               bool& have, VertexCell& out) {
     unsigned int pending = __ballot_sync(0xffffffffu, act);
     while (pending) {
         const int leader = __ffs(pending) - 1;
-        const unsigned long long lb = __shfl_sync(0xffffffffu, myb, leader);
-        if ((long long)lb != bb) {
-            bbase = __shfl_sync(0xffffffffu, mybase, leader);
-            bcount = __shfl_sync(0xffffffffu, mycnt, leader);
-            bb = (long long)lb;
-            load_block(V, S, warp, lane, lb);
+        const uint32_t vl = __shfl_sync(0xffffffffu, v, leader);
+        if (!have || vl < bbase || vl - bbase >= bcount) {
+            descend(V, S, vl, bb, bbase, bcount);  // uniform across the warp
+            load_block(V, S, warp, lane, bb);
+            have = true;
         }
-        const bool mine = ((pending >> lane) & 1u) && myb == (unsigned long long)bb;
-        if (mine) out = find_cell(V, S, warp, (unsigned long long)bb, (unsigned int)(v - bbase));
+        const bool mine = ((pending >> lane) & 1u) && v >= bbase && v - bbase < bcount;
+        if (mine) out = find_cell(V, S, warp, bb, v - bbase);
         pending &= ~__ballot_sync(0xffffffffu, mine);
         __syncwarp();
     }
@@ -194,67 +178,33 @@ __device__ __forceinline__ EdgeGeom edge_of(const TraverseSmem& S, const VertexC
 
 // ---------------------------------------------------------------------------
 template <int FT, int MODE>
-__global__ void __launch_bounds__(kThreads) traverse_kernel(const __grid_constant__ Volume V,
-                                                            const __grid_constant__ TraverseOut O) {
+__global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_constant__ Volume V,
+                                                               const __grid_constant__ TraverseOut O) {
     __shared__ __align__(16) TraverseSmem S;
     load_tables(V, S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long total = V.ctrl->total;
-    const unsigned long long N = total < O.capacity ? total : O.capacity;
+    const uint32_t N = (uint32_t)(total < O.capacity ? total : O.capacity);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (total > O.capacity) atomicOr(&V.ctrl->status, kStatusCapacity);
-        V.ctrl->written = (unsigned int)N;
+        V.ctrl->written = N;
     }
-    const float iso = V.iso;
-    constexpr unsigned long long VW = 32ull * kTraverseRounds;
-    const unsigned long long nchunks = (N + VW - 1) / VW;
-    long long bb = -1;
-    unsigned long long bbase = 0;
-    unsigned int bcount = 0;
-    for (unsigned long long chunk = (unsigned long long)blockIdx.x * kWarps + warp; chunk < nchunks;
-         chunk += (unsigned long long)gridDim.x * kWarps) {
+    constexpr uint32_t VW = 32u * kTraverseRounds;
+    const uint32_t nchunks = (N + VW - 1) / VW;
+    uint32_t bb = 0, bbase = 0, bcount = 0;
+    bool have = false;
+    for (uint32_t chunk = blockIdx.x * kWarps + warp; chunk < nchunks; chunk += gridDim.x * kWarps) {
 #pragma unroll 1
         for (int r = 0; r < kTraverseRounds; r++) {
-            const unsigned long long v = chunk * VW + 32ull * r + lane;
+            const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
             VertexCell c;
-            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, c)) continue;
+            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, have, c)) continue;
             const EdgeGeom g = edge_of(S, c);
-            const int ax = g.axis;
-            float t, n[3];
-            if (MODE == kModeBinary) {
-                t = 0.5f;
-                const float* bn = g_binary_normals + 3 * (16 * c.code + c.k);
-                n[0] = bn[0]; n[1] = bn[1]; n[2] = bn[2];
-            } else {
-                const int* a = g.a;
-                const int b[3] = {a[0] + (ax == 0), a[1] + (ax == 1), a[2] + (ax == 2)};
-                const float va = fetch<FT>(V, a[0], a[1], a[2]);
-                const float vb = fetch<FT>(V, b[0], b[1], b[2]);
-                t = (va - iso) / (va - vb);
-                const float omt = 1.0f - t;
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    const int ex = (i == 0), ey = (i == 1), ez = (i == 2);
-                    const float fa_p = (i == ax) ? vb : fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
-                    const float fb_p = fetch<FT>(V, b[0] + ex, b[1] + ey, b[2] + ez);
-                    if (MODE == kModeForward) {
-                        // iso - lerp(f(a+e), f(b+e), t), differences first
-                        n[i] = omt * (iso - fa_p) + t * (iso - fb_p);
-                    } else {
-                        const float fa_m = fetch<FT>(V, a[0] - ex, a[1] - ey, a[2] - ez);
-                        const float fb_m = (i == ax) ? va : fetch<FT>(V, b[0] - ex, b[1] - ey, b[2] - ez);
-                        n[i] = -0.5f * (omt * (fa_p - fa_m) + t * (fb_p - fb_m));
-                    }
-                }
-            }
-            float p[3];
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-                p[i] = ((float)g.a[i] + (i == ax ? t : 0.0f)) * V.scale[i];
-                n[i] *= V.scale[i];
-            }
+            float p[3], n[3], t;
+            edge_vertex<FT, MODE>(V, g.a, g.axis, c.x, c.y, c.z, g_binary_normals + 3 * (16 * c.code + c.k), p, n,
+                                  t);
             const unsigned long long o = V.vertex_base + v;
             if (O.pos) __stcs(O.pos + o, make_float4(p[0], p[1], p[2], 1.0f));
             if (O.nrm) __stcs(O.nrm + o, make_float4(n[0], n[1], n[2], 0.0f));
@@ -280,80 +230,78 @@ __global__ void __launch_bounds__(kThreads) traverse_kernel(const __grid_constan
 //   central: n_i = -1/2((1-t)(f(a+e_i) - f(a-e_i)) + t(f(b+e_i) - f(b-e_i))) s_i
 // Clamped samples scatter to the sample that was read.
 namespace {
-template <int FT>
-__device__ __forceinline__ void scatter(const Volume& V, float* dfield, int x, int y, int z, float g) {
-    x = min(max(x, 0), V.lattice[0] - 1);
-    y = min(max(y, 0), V.lattice[1] - 1);
-    z = min(max(z, 0), V.lattice[2] - 1);
+__device__ __forceinline__ void scatter(const Volume& V, float* dfield, const int* a, int dx, int dy, int dz,
+                                        float g) {
+    const int x = min(max(a[0] + dx, 0), V.lattice[0] - 1);
+    const int y = min(max(a[1] + dy, 0), V.lattice[1] - 1);
+    const int z = min(max(a[2] + dz, 0), V.lattice[2] - 1);
     atomicAdd(dfield + (long long)z * V.slice_pitch + (long long)y * V.row_pitch + x, g);
 }
 }  // namespace
 
 template <int FT, int MODE>
-__global__ void __launch_bounds__(kThreads) adjoint_kernel(const __grid_constant__ Volume V,
-                                                           const __grid_constant__ AdjointIO A) {
+__global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_constant__ Volume V,
+                                                              const __grid_constant__ AdjointIO A) {
     __shared__ __align__(16) TraverseSmem S;
     load_tables(V, S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long total = V.ctrl->total;
-    const unsigned long long N = total < A.count ? total : A.count;
+    const uint32_t N = (uint32_t)(total < A.count ? total : A.count);
     const float iso = V.iso;
-    constexpr unsigned long long VW = 32ull * kTraverseRounds;
-    const unsigned long long nchunks = (N + VW - 1) / VW;
-    long long bb = -1;
-    unsigned long long bbase = 0;
-    unsigned int bcount = 0;
-    for (unsigned long long chunk = (unsigned long long)blockIdx.x * kWarps + warp; chunk < nchunks;
-         chunk += (unsigned long long)gridDim.x * kWarps) {
+    constexpr uint32_t VW = 32u * kTraverseRounds;
+    const uint32_t nchunks = (N + VW - 1) / VW;
+    uint32_t bb = 0, bbase = 0, bcount = 0;
+    bool have = false;
+    for (uint32_t chunk = blockIdx.x * kWarps + warp; chunk < nchunks; chunk += gridDim.x * kWarps) {
 #pragma unroll 1
         for (int r = 0; r < kTraverseRounds; r++) {
-            const unsigned long long v = chunk * VW + 32ull * r + lane;
+            const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
             VertexCell c;
-            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, c)) continue;
+            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, have, c)) continue;
             const EdgeGeom g = edge_of(S, c);
             const int ax = g.axis;
-            const int* a = g.a;
-            const int b[3] = {a[0] + (ax == 0), a[1] + (ax == 1), a[2] + (ax == 2)};
+            const int ex = ax == 0, ey = ax == 1, ez = ax == 2;
+            const EdgeSamples<FT> f(V, g.a, ax, c.x, c.y, c.z);
             const unsigned long long o = V.vertex_base + v;
             const float4 dp = A.dpos ? __ldg(A.dpos + o) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 dn = A.dnrm ? __ldg(A.dnrm + o) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float dpv[3] = {dp.x, dp.y, dp.z};
             const float dnv[3] = {dn.x * V.scale[0], dn.y * V.scale[1], dn.z * V.scale[2]};
-            const float va = fetch<FT>(V, a[0], a[1], a[2]);
-            const float vb = fetch<FT>(V, b[0], b[1], b[2]);
+            const float va = f.fa(), vb = f.fb();
             const float den = va - vb;
-            const float t = (va - iso) / den;
+            const FF tf = ff_ratio_of_diffs(va, iso, va, vb);
+            const float t = tf.hi + tf.lo;
             const float omt = 1.0f - t;
             float dLdt = dpv[ax] * V.scale[ax];
             float ga = 0.0f, gb = 0.0f;  // direct contributions to samples a and b
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                const int ex = (i == 0), ey = (i == 1), ez = (i == 2);
-                const float fa_p = (i == ax) ? vb : fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
-                const float fb_p = fetch<FT>(V, b[0] + ex, b[1] + ey, b[2] + ez);
+                const int dx = i == 0, dy = i == 1, dz = i == 2;
+                const float fa_p = (i == ax) ? vb : f.fa_plus(i);
+                const float fb_p = f.fb_plus(i);
                 if (MODE == kModeForward) {
                     dLdt += dnv[i] * (fa_p - fb_p);
                     const float wa = -omt * dnv[i], wb = -t * dnv[i];
-                    if (i == ax) gb += wa; else scatter<FT>(V, A.dfield, a[0] + ex, a[1] + ey, a[2] + ez, wa);
-                    scatter<FT>(V, A.dfield, b[0] + ex, b[1] + ey, b[2] + ez, wb);
+                    if (i == ax) gb += wa; else scatter(V, A.dfield, g.a, dx, dy, dz, wa);
+                    scatter(V, A.dfield, g.a, ex + dx, ey + dy, ez + dz, wb);
                 } else {
-                    const float fa_m = fetch<FT>(V, a[0] - ex, a[1] - ey, a[2] - ez);
-                    const float fb_m = (i == ax) ? va : fetch<FT>(V, b[0] - ex, b[1] - ey, b[2] - ez);
+                    const float fa_m = f.fa_minus(i);
+                    const float fb_m = (i == ax) ? va : f.fb_minus(i);
                     dLdt += -0.5f * dnv[i] * ((fb_p - fb_m) - (fa_p - fa_m));
                     const float wa = -0.5f * omt * dnv[i], wb = -0.5f * t * dnv[i];
-                    if (i == ax) gb += wa; else scatter<FT>(V, A.dfield, a[0] + ex, a[1] + ey, a[2] + ez, wa);
-                    scatter<FT>(V, A.dfield, a[0] - ex, a[1] - ey, a[2] - ez, -wa);
-                    scatter<FT>(V, A.dfield, b[0] + ex, b[1] + ey, b[2] + ez, wb);
-                    if (i == ax) ga -= wb; else scatter<FT>(V, A.dfield, b[0] - ex, b[1] - ey, b[2] - ez, -wb);
+                    if (i == ax) gb += wa; else scatter(V, A.dfield, g.a, dx, dy, dz, wa);
+                    scatter(V, A.dfield, g.a, -dx, -dy, -dz, -wa);
+                    scatter(V, A.dfield, g.a, ex + dx, ey + dy, ez + dz, wb);
+                    if (i == ax) ga -= wb; else scatter(V, A.dfield, g.a, ex - dx, ey - dy, ez - dz, -wb);
                 }
             }
             const float inv = 1.0f / (den * den);
             ga += dLdt * (iso - vb) * inv;
             gb += dLdt * (va - iso) * inv;
-            scatter<FT>(V, A.dfield, a[0], a[1], a[2], ga);
-            scatter<FT>(V, A.dfield, b[0], b[1], b[2], gb);
+            scatter(V, A.dfield, g.a, 0, 0, 0, ga);
+            scatter(V, A.dfield, g.a, ex, ey, ez, gb);
         }
     }
 }
@@ -362,11 +310,11 @@ __global__ void __launch_bounds__(kThreads) adjoint_kernel(const __grid_constant
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st) {
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
-#define HPMC_TRAVERSE_CASE(FT_)                                                                   \
-    case FT_:                                                                                     \
-        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, 0, st>>>(V, O); \
+#define HPMC_TRAVERSE_CASE(FT_)                                                                        \
+    case FT_:                                                                                          \
+        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, 0, st>>>(V, O);   \
         else if (mode == kModeCentral) traverse_kernel<FT_, kModeCentral><<<grid, kThreads, 0, st>>>(V, O); \
-        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, 0, st>>>(V, O);                \
+        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, 0, st>>>(V, O);                     \
         break;
     switch (V.ftype) {
         HPMC_TRAVERSE_CASE(kFieldF32)
@@ -399,10 +347,6 @@ cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode,
     }
     return cudaGetLastError();
 }
-
-}  // namespace hpmc
-
-namespace hpmc {
 
 int traverse_blocks_per_sm() {
     int n = 0;

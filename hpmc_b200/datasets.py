@@ -53,7 +53,7 @@ def noise_u8(n: int = 256, seed: int = 1, sigma: float = 3.0):
     g = np.exp(-2.0 * (np.pi * sigma) ** 2 * k * k)  # Fourier transform of the Gaussian
     U = np.fft.rfftn(u)
     U *= g[:, None, None] * g[None, :, None] * g[None, None, : n // 2 + 1]
-    s = np.fft.irfftn(U, s=u.shape)
+    s = np.fft.irfftn(U, s=u.shape, axes=(0, 1, 2))
     lo, hi = s.min(), s.max()
     v = np.rint((s - lo) * (255.0 / (hi - lo)))
     return v.astype(np.uint8), 128.0

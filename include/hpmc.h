@@ -237,6 +237,11 @@ int HPMCsetTraversalDebugBuffers(struct HPMCTraversalHandle* th, int32_t* cell_i
  * 4 arena, 8 timeout); waits for the handle's stream. */
 int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
 
+/* Classification path of the last build: 1 = TMA column kernel (every 32x32
+ * cell block inside one slice tile, 16-byte aligned array field), 0 = generic
+ * per-block kernel (narrow tiles, unaligned pitches, functor fields). */
+int HPMCgetClassifyPath(struct HPMCHistoPyramid* h, int* path);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -40,6 +40,7 @@ def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=Fals
     hp.build(iso)
     n = hp.acquire_number_of_vertices()
     assert hp.last_error == 0, hp.last_error
+    path = hp.classify_path()
     levels = {}
     jtop = max(5, L[4] + 1)
     for j in range(5, jtop + 1):
@@ -54,7 +55,7 @@ def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=Fals
     written = th.extract_to(pos, nrm, n)
     status = hp.device_status()
     torch.cuda.synchronize()
-    out = dict(n=n, written=written, layout=L, levels=levels, status=status,
+    out = dict(n=n, written=written, layout=L, levels=levels, status=status, path=path,
                pos=pos[:n].cpu().numpy(), nrm=nrm[:n].cpu().numpy(), info=info[:n].cpu().numpy(),
                t=tt[:n].cpu().numpy())
     if capture_codes:

@@ -53,6 +53,32 @@ def test_random_lattices(hpmc, oracle, shape, dtype):
     compare(g, e)
 
 
+TMA_SHAPES = [(2, 50, 36), (7, 65, 68), (33, 31, 40), (100, 33, 64), (40, 40, 48), (2, 64, 64), (9, 100, 96),
+              (70, 200, 144)]
+
+
+@pytest.mark.parametrize("shape", TMA_SHAPES)
+@pytest.mark.parametrize("dtype", ["f32", "u8", "unorm8"])
+def test_tma_column_path(hpmc, oracle, shape, dtype):
+    """Aligned fields whose 32x32 blocks lie inside one slice tile take the TMA
+    column kernel (odd cell counts, single-slice volumes, partial footprints)."""
+    rng = np.random.default_rng(sum(shape) * 3 + len(dtype))
+    if dtype == "f32":
+        field = rng.normal(size=shape).astype(np.float32)
+        field[rng.random(shape) < 0.05] = 0.0
+        iso = 0.0
+    else:
+        field = rng.integers(100, 156, size=shape).astype(np.uint8)
+        iso = 128.0 if dtype == "u8" else 128.0 / 255.0
+    unorm = dtype == "unorm8"
+    g = run_gpu(hpmc, field, iso, unorm=unorm)
+    L = oracle.layout((shape[2], shape[1], shape[0]))
+    expect_tma = 2 * L.tile[0] >= 32 and 2 * L.tile[1] >= 32 and (shape[2] * field.itemsize) % 16 == 0
+    assert g["path"] == (1 if expect_tma else 0)
+    e = oracle_expect(oracle, field, iso, unorm=unorm)
+    compare(g, e)
+
+
 @pytest.mark.parametrize("pad", [1, 3, 16])
 def test_pitched_fields_take_generic_path_identically(hpmc, oracle, pad):
     rng = np.random.default_rng(pad)
