@@ -189,6 +189,7 @@ int bind_field(HPMCHistoPyramid* h) {
                                          : hpmc::kFieldUNorm8;
     V.row_pitch = (long long)(rp / es);
     V.slice_pitch = (long long)(sp / es);
+    V.idx32 = (V.slice_pitch * ((long long)h->lattice[2] + 1) < (1ll << 31)) ? 1 : 0;
     // TMA column path: column layout, 16-byte aligned base and pitches
     h->have_tmap = false;
     if (V.column_layout && ((uintptr_t)f.ptr % 16 == 0) && rp % 16 == 0 && sp % 16 == 0) {

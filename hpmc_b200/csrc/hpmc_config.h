@@ -14,7 +14,7 @@ constexpr int kWarps = kThreads / 32;
 // Classification: sample layers per TMA box (one ring stage), ring depth, and
 // the slices per column CTA (chosen per volume from kColumnSliceChoices so
 // that slices + 1 layers fill whole boxes and the grid covers the GPU).
-constexpr int kLayersPerBox = 4;
+constexpr int kLayersPerBox = 8;
 constexpr int kRingStages = 2;
 constexpr int kColumnSliceChoices[4] = {63, 31, 15, 7};
 
@@ -22,7 +22,7 @@ constexpr int kColumnSliceChoices[4] = {63, 31, 15, 7};
 // (levels with <= 1024 entries: 1 + 4 + ... + 1024, each padded to 4).
 constexpr int kTopCacheEntries = 1368;
 // Vertices per warp work item (R rounds of 32).
-constexpr int kTraverseRounds = 16;
+constexpr int kTraverseRounds = 8;
 
 // Bounded waits: an mbarrier poll gives up after this long (a TMA box lands
 // in microseconds; only a fault in the copy path gets near it).

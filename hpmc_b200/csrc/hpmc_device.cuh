@@ -51,6 +51,8 @@ struct Ctrl {
     unsigned int reduce_done;    // last-block-done counter of the reduce kernel
     unsigned int status;         // sticky error bits (kStatus*)
     unsigned int written;        // vertices written by the last extraction
+    unsigned int work_next;      // traversal work queue: next chunk to hand out
+    unsigned int work_done;      // traversal CTAs finished (the last one resets the queue)
     unsigned int active_blocks;  // non-empty blocks of the last build
     unsigned int pad;
 };
@@ -75,6 +77,7 @@ struct Volume {
     const void* field;
     long long row_pitch;     // elements
     long long slice_pitch;   // elements
+    int idx32;               // every element index (+ one slice) fits in int32
     int ftype;
     int lattice[3];
     int cells[3];
@@ -130,6 +133,15 @@ __host__ __device__ __forceinline__ uint64_t morton_spread(uint64_t v) {
     v = (v | (v << 1)) & 0x5555555555555555ull;
     return v;
 }
+// 16-bit value -> even bits of a 32-bit word
+__host__ __device__ __forceinline__ uint32_t morton_spread16(uint32_t v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
 // 10-bit Morton index inside a block -> (cx, cy) in 0..31
 __host__ __device__ __forceinline__ void morton10(uint32_t m, int& cx, int& cy) {
     uint32_t x = m & 0x155u, y = (m >> 1) & 0x155u;
@@ -178,7 +190,7 @@ __host__ __device__ __forceinline__ uint64_t column_block_index(const Volume& V,
     const uint32_t tu = (uint32_t)z & ((1u << V.lx_l2) - 1u), tv = (uint32_t)z >> V.lx_l2;
     const uint32_t X0 = (tu << V.wx_l2) + 32u * (uint32_t)fx;
     const uint32_t Y0 = (tv << V.wy_l2) + 32u * (uint32_t)fy;
-    return morton_spread(X0 >> 5) | (morton_spread(Y0 >> 5) << 1);
+    return (uint64_t)(morton_spread16(X0 >> 5) | (morton_spread16(Y0 >> 5) << 1));
 }
 
 }  // namespace hpmc

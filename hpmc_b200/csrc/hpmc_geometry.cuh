@@ -61,50 +61,76 @@ __device__ __forceinline__ float ff_lerp(FF A, FF B, FF t) {
 // Integer lattice index -> float without the conversion pipe (0 <= v < 2^23).
 __device__ __forceinline__ float index_to_float(int v) { return __int_as_float(0x4B000000 | v) - 8388608.0f; }
 
-// Samples around edge end point a: interior cells (all samples inside the
-// lattice) read through precomputed element offsets, others clamp each
-// coordinate (GL_CLAMP + NEAREST).  Functor fields evaluate the functor.
-template <int FT>
-struct EdgeSamples {
-    const Volume& V;
-    int a[3];
-    int ex, ey, ez;            // a -> b
-    long long base, ob;        // element index of a; offset a -> b
-    long long o[3];            // offsets of +x, +y, +z
-    bool interior;
-    __device__ __forceinline__ EdgeSamples(const Volume& Vv, const int* aa, int axis, int cx, int cy, int cz)
-        : V(Vv) {
-        a[0] = aa[0];
-        a[1] = aa[1];
-        a[2] = aa[2];
-        ex = axis == 0;
-        ey = axis == 1;
-        ez = axis == 2;
-        // samples span cell-1 .. cell+3 on each axis
-        interior = FT != kFieldFunctor && cx >= 1 && cx <= V.lattice[0] - 4 && cy >= 1 &&
-                   cy <= V.lattice[1] - 4 && cz >= 1 && cz <= V.lattice[2] - 4;
-        o[0] = 1;
-        o[1] = V.row_pitch;
-        o[2] = V.slice_pitch;
-        base = (long long)a[2] * V.slice_pitch + (long long)a[1] * V.row_pitch + a[0];
-        ob = axis == 0 ? o[0] : axis == 1 ? o[1] : o[2];
-    }
-    // f(a + (dx,dy,dz)) given the matching element offset
-    __device__ __forceinline__ float at(int dx, int dy, int dz, long long off) const {
-        if (FT != kFieldFunctor && interior) return fetch_raw<FT>(V, base + off);
-        return fetch<FT>(V, a[0] + dx, a[1] + dy, a[2] + dz);
-    }
-    __device__ __forceinline__ float fa() const { return at(0, 0, 0, 0); }
-    __device__ __forceinline__ float fb() const { return at(ex, ey, ez, ob); }
-    __device__ __forceinline__ float fa_plus(int i) const { return at(i == 0, i == 1, i == 2, o[i]); }
-    __device__ __forceinline__ float fa_minus(int i) const { return at(-(i == 0), -(i == 1), -(i == 2), -o[i]); }
-    __device__ __forceinline__ float fb_plus(int i) const {
-        return at(ex + (i == 0), ey + (i == 1), ez + (i == 2), ob + o[i]);
-    }
-    __device__ __forceinline__ float fb_minus(int i) const {
-        return at(ex - (i == 0), ey - (i == 1), ez - (i == 2), ob - o[i]);
-    }
+// The field samples one vertex reads around its edge a -> b = a + e_axis:
+// f(a), f(b), f(a +- e_i), f(b +- e_i).  All loads of a vertex are issued in
+// one branch-free block: interior cells (every sample inside the lattice)
+// through precomputed element offsets, boundary cells with each coordinate
+// clamped (GL_CLAMP + NEAREST), functor fields by evaluating the functor.
+struct EdgeField {
+    float va, vb;
+    float ap[3], bp[3];  // f(a + e_i), f(b + e_i)
+    float am[3], bm[3];  // f(a - e_i), f(b - e_i)   (central differences only)
 };
+
+template <int FT, bool CENTRAL>
+__device__ __forceinline__ void gather_edge(const Volume& V, const int* a, int axis, int cx, int cy, int cz,
+                                            EdgeField& F) {
+    const int ex = axis == 0, ey = axis == 1, ez = axis == 2;
+    // samples span cell-1 .. cell+3 on each axis
+    const bool interior = FT != kFieldFunctor && cx >= 1 && cx <= V.lattice[0] - 4 && cy >= 1 &&
+                          cy <= V.lattice[1] - 4 && cz >= 1 && cz <= V.lattice[2] - 4;
+    if (FT != kFieldFunctor && interior && V.idx32) {
+        // 32-bit element offsets from the sample at a (one wide address each)
+        using T = typename std::conditional<FT == kFieldF32, float, unsigned char>::type;
+        const int o[3] = {1, (int)V.row_pitch, (int)V.slice_pitch};
+        const T* pa = static_cast<const T*>(V.field) + (a[2] * o[2] + a[1] * o[1] + a[0]);
+        const T* pb = pa + (axis == 0 ? o[0] : axis == 1 ? o[1] : o[2]);
+        auto ld = [](const T* p) -> float {
+            if constexpr (FT == kFieldF32) return __ldg(p);
+            else if constexpr (FT == kFieldU8) return u8_to_float(__ldg(p));
+            else return unorm8_to_float(__ldg(p));
+        };
+        F.va = ld(pa);
+        F.vb = ld(pb);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            F.ap[i] = ld(pa + o[i]);
+            F.bp[i] = ld(pb + o[i]);
+            if (CENTRAL) {
+                F.am[i] = ld(pa - o[i]);
+                F.bm[i] = ld(pb - o[i]);
+            }
+        }
+    } else if (FT != kFieldFunctor && interior) {
+        const long long o[3] = {1ll, V.row_pitch, V.slice_pitch};
+        const long long pa = (long long)a[2] * V.slice_pitch + (long long)a[1] * V.row_pitch + a[0];
+        const long long pb = pa + (axis == 0 ? o[0] : axis == 1 ? o[1] : o[2]);
+        F.va = fetch_raw<FT>(V, pa);
+        F.vb = fetch_raw<FT>(V, pb);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            F.ap[i] = fetch_raw<FT>(V, pa + o[i]);
+            F.bp[i] = fetch_raw<FT>(V, pb + o[i]);
+            if (CENTRAL) {
+                F.am[i] = fetch_raw<FT>(V, pa - o[i]);
+                F.bm[i] = fetch_raw<FT>(V, pb - o[i]);
+            }
+        }
+    } else {
+        F.va = fetch<FT>(V, a[0], a[1], a[2]);
+        F.vb = fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const int dx = i == 0, dy = i == 1, dz = i == 2;
+            F.ap[i] = fetch<FT>(V, a[0] + dx, a[1] + dy, a[2] + dz);
+            F.bp[i] = fetch<FT>(V, a[0] + ex + dx, a[1] + ey + dy, a[2] + ez + dz);
+            if (CENTRAL) {
+                F.am[i] = fetch<FT>(V, a[0] - dx, a[1] - dy, a[2] - dz);
+                F.bm[i] = fetch<FT>(V, a[0] + ex - dx, a[1] + ey - dy, a[2] + ez - dz);
+            }
+        }
+    }
+}
 
 enum { kGeomForward = 0, kGeomCentral = 1, kGeomBinary = 2 };
 
@@ -128,22 +154,20 @@ __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int a
         n[1] = binary_normal[1];
         n[2] = binary_normal[2];
     } else {
-        const EdgeSamples<FT> f(V, a, axis, cx, cy, cz);
+        EdgeField F;
+        gather_edge<FT, MODE == kGeomCentral>(V, a, axis, cx, cy, cz, F);
         const float iso = V.iso;
-        const float va = f.fa(), vb = f.fb();
-        t = (va - iso) / (va - vb);  // (f(a) - iso) / (f(a) - f(b)), relative error <= 3u
+        t = (F.va - iso) / (F.va - F.vb);  // (f(a) - iso) / (f(a) - f(b)), relative error <= 3u
         float s2 = 0.0f, n2 = 0.0f;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            const float fap = (i == axis) ? vb : f.fa_plus(i);
-            const float fbp = f.fb_plus(i);
             float A, B;
             if (MODE == kGeomForward) {
-                A = iso - fap;
-                B = iso - fbp;
+                A = iso - F.ap[i];
+                B = iso - F.bp[i];
             } else {
-                A = fap - f.fa_minus(i);
-                B = fbp - ((i == axis) ? va : f.fb_minus(i));
+                A = F.ap[i] - F.am[i];
+                B = F.bp[i] - F.bm[i];
             }
             n[i] = fmaf(t, B - A, A);
             const float s = fabsf(A) + fabsf(B);
@@ -152,18 +176,13 @@ __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int a
         }
         if (s2 > 23.0f * n2) {
             // ill-conditioned: float-float crossing parameter and lerps
-            const FF tf = ff_ratio_of_diffs(va, iso, va, vb);
+            const FF tf = ff_ratio_of_diffs(F.va, iso, F.va, F.vb);
 #pragma unroll
             for (int i = 0; i < 3; i++) {
-                const float fap = (i == axis) ? vb : f.fa_plus(i);
-                const float fbp = f.fb_plus(i);
-                if (MODE == kGeomForward) {
-                    n[i] = ff_lerp(two_sum(iso, -fap), two_sum(iso, -fbp), tf);
-                } else {
-                    const float fam = f.fa_minus(i);
-                    const float fbm = (i == axis) ? va : f.fb_minus(i);
-                    n[i] = ff_lerp(two_sum(fap, -fam), two_sum(fbp, -fbm), tf);
-                }
+                if (MODE == kGeomForward)
+                    n[i] = ff_lerp(two_sum(iso, -F.ap[i]), two_sum(iso, -F.bp[i]), tf);
+                else
+                    n[i] = ff_lerp(two_sum(F.ap[i], -F.am[i]), two_sum(F.bp[i], -F.bm[i]), tf);
             }
             t = tf.hi + tf.lo;
         }

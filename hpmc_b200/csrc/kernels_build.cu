@@ -116,45 +116,47 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
                                                     uint32_t vmask, const uint32_t* rows_b, uint64_t col_b,
                                                     const uint32_t* rows_t, uint64_t col_t,
                                                     const uint8_t* s_cnt) {
-    // 33-bit rows y and y+1 of both layers (bit 32 = column x0+32)
-    const uint64_t A0 = rows_b[lane] | (((col_b >> lane) & 1ull) << 32);
-    const uint64_t A1 = rows_b[lane + 1] | (((col_b >> (lane + 1)) & 1ull) << 32);
-    const uint64_t B0 = rows_t[lane] | (((col_t >> lane) & 1ull) << 32);
-    const uint64_t B1 = rows_t[lane + 1] | (((col_t >> (lane + 1)) & 1ull) << 32);
+    // rows y and y+1 of both layers; bit 32 of a row (column x0+32) comes
+    // from the column word: (row >> 1) | colbit << 31 is the row shifted by one cell
+    const uint32_t cbl = (uint32_t)col_b, cbh = (uint32_t)(col_b >> 32);
+    const uint32_t ctl = (uint32_t)col_t, cth = (uint32_t)(col_t >> 32);
+    const uint32_t a0 = rows_b[lane], a1 = rows_b[lane + 1];
+    const uint32_t b0 = rows_t[lane], b1 = rows_t[lane + 1];
     uint32_t c[8];
-    c[0] = (uint32_t)A0;         // (x,   y,   z)
-    c[1] = (uint32_t)(A0 >> 1);  // (x+1, y,   z)
-    c[2] = (uint32_t)A1;         // (x,   y+1, z)
-    c[3] = (uint32_t)(A1 >> 1);
-    c[4] = (uint32_t)B0;         // (x,   y,   z+1)
-    c[5] = (uint32_t)(B0 >> 1);
-    c[6] = (uint32_t)B1;
-    c[7] = (uint32_t)(B1 >> 1);
+    c[0] = a0;                                                   // (x,   y,   z)
+    c[1] = (a0 >> 1) | (((cbl >> lane) & 1u) << 31);             // (x+1, y,   z)
+    c[2] = a1;                                                   // (x,   y+1, z)
+    c[3] = (a1 >> 1) | ((__funnelshift_rc(cbl, cbh, lane + 1) & 1u) << 31);
+    c[4] = b0;                                                   // (x,   y,   z+1)
+    c[5] = (b0 >> 1) | (((ctl >> lane) & 1u) << 31);
+    c[6] = b1;
+    c[7] = (b1 >> 1) | ((__funnelshift_rc(ctl, cth, lane + 1) & 1u) << 31);
     uint32_t all = c[0], any = c[0];
 #pragma unroll
     for (int k = 1; k < 8; k++) {
         all &= c[k];
         any |= c[k];
     }
-    uint32_t active = (all ^ any) & vmask;
-    uint32_t cnt = 0;
-    while (active) {
-        const int x = __ffs(active) - 1;
-        uint32_t code = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) code |= ((c[k] >> x) & 1u) << k;
-        cnt += s_cnt[code];
-        active &= active - 1;
-    }
-    const uint32_t total = __reduce_add_sync(0xffffffffu, cnt);
+    // cells that are neither all-inside nor all-outside: the only ones with vertices
+    const bool has_vertices = __any_sync(0xffffffffu, ((all ^ any) & vmask) != 0u);
     const uint64_t b = column_block_index(V, z, fx, fy);
-    if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-    if (total == 0 && !V.codes_out) return;
+    if (!has_vertices) {
+        if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = 0u;
+        if (!V.codes_out) return;
+    }
     // codes of this row (cells outside the grid are masked to 0)
 #pragma unroll
     for (int k = 0; k < 8; k++) c[k] &= vmask;
     uint32_t w[8];
     slices_to_codes(c, w);
+    uint32_t total = 0;
+    if (has_vertices) {
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int i = 0; i < 32; i++) cnt += s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        total = __reduce_add_sync(0xffffffffu, cnt);
+        if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
+    }
     if (total) {
         // arena word for quad (qx, qy) = cells (2qx,2qy),(2qx+1,2qy),(2qx,2qy+1),(2qx+1,2qy+1):
         // rows 2qy (even lane) and 2qy+1 (odd lane); even lanes store qx 0..7, odd 8..15
@@ -205,8 +207,8 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     // (the launch reserves 128 spare bytes)
     uint8_t* const s_ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
     __shared__ __align__(8) uint64_t s_bar[kRingStages];
-    __shared__ __align__(16) uint32_t s_rows[8][36];  // layer % 8: bit x = sample (x0 + x, y0 + r) below iso
-    __shared__ uint64_t s_col[8];       // layer % 8: bit r = sample (x0 + 32, y0 + r) below iso
+    __shared__ __align__(16) uint32_t s_rows[16][36];  // layer % 16: bit x = sample (x0 + x, y0 + r) below iso
+    __shared__ uint64_t s_col[16];                      // layer % 16: bit r = sample (x0 + 32, y0 + r) below iso
     __shared__ uint8_t s_cnt[256];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -241,27 +243,24 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     for (; k < nbox; k++) {
         const int s = k % kRingStages;
         const uint32_t parity = (uint32_t)(k / kRingStages) & 1u;
-        // one warp polls the box's barrier; the others wait at the CTA barrier
-        if (warp == 0 && !mbar_wait_bounded(&s_bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout))
-            timed_out = true;
-        if (__syncthreads_or(timed_out)) break;
-        if (warp != 0) mbar_try_wait(&s_bar[s], parity);  // completed phase: acquire the TMA writes
         const int lb = k * kLayersPerBox;
         const int nl = min(kLayersPerBox, nlayers - lb);
+        // every warp waits on the box's mbarrier (suspended in hardware, not spinning)
+        if (!mbar_wait_bounded(&s_bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout)) timed_out = true;
         const T* st = reinterpret_cast<const T*>(s_ring + s * STAGE_STRIDE);
 #pragma unroll
         for (int l = 0; l < kLayersPerBox; l++) {
-            if (l < nl) {
+            if (l < nl && !timed_out) {
                 // warp w: rows 4w .. 4w+3 (one ballot per row, one 16-byte store)
                 const T* layer = st + l * LAYER;
-                const int buf = (lb + l) & 7;
+                const int buf = (lb + l) & 15;
                 const T* row = layer + 4 * warp * BXE + lane;
                 const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(row[0], iso, u8_thr));
                 const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(row[BXE], iso, u8_thr));
                 const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(row[2 * BXE], iso, u8_thr));
                 const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(row[3 * BXE], iso, u8_thr));
                 if (lane == 0) *reinterpret_cast<uint4*>(&s_rows[buf][4 * warp]) = make_uint4(b0, b1, b2, b3);
-                if (warp == kWarps - 1 - l) {  // row 32 and column x0+32
+                if (warp == ((lb + l + 3) & 7)) {  // row 32 and column x0+32 (a warp not classifying)
                     const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(layer[32 * BXE + lane], iso, u8_thr));
                     const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(layer[lane * BXE + 32], iso, u8_thr));
                     const bool corner = below<FT>(layer[32 * BXE + 32], iso, u8_thr);
@@ -272,16 +271,20 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
                 }
             }
         }
-        __syncthreads();  // stage s consumed; bit rows of layers lb .. lb+nl-1 ready
+        // the only CTA barrier of a box: stage s consumed, bit rows of layers
+        // lb .. lb+nl-1 ready, and a uniform decision on a timed-out wait
+        if (__syncthreads_or(timed_out)) break;
         if (tid == 0 && k + kRingStages < nbox) {
             mbar_arrive_expect_tx(&s_bar[s], STAGE_BYTES);
             tma_load_3d(s_ring + s * STAGE_STRIDE, &tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox, &s_bar[s]);
         }
-        // slices whose upper layer arrived in this box, one warp each; row
-        // buffers of a layer stay untouched until two boxes later
-        const int sl = lb - 1 + warp;  // slice (local) = its lower layer
-        if (warp < nl && sl >= 0) {
-            const int bb = sl & 7, bt = (sl + 1) & 7;
+        // slices whose upper layer arrived in this box, warp (slice mod 8) each,
+        // so the work rotates over the warps from box to box.  A warp may still
+        // classify box k while others convert box k+1: row buffers (layer mod 16)
+        // of box k are not rewritten before box k+4.
+        const int sl = lb - 1 + ((warp - (lb - 1)) & 7);  // the slice of this warp, if any
+        if (sl >= 0 && sl <= lb + nl - 2) {
+            const int bb = sl & 15, bt = (sl + 1) & 15;
             classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, s_rows[bb], s_col[bb], s_rows[bt], s_col[bt],
                                 s_cnt);
         }

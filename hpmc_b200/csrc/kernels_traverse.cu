@@ -45,13 +45,38 @@ struct TraverseSmem {
     uint32_t codew[kWarps][kBlockWords];
     uint16_t pref[kWarps][kBlockKeys];
     uint32_t top[kTopCacheEntries];
+    uint16_t morton[kBlockKeys];  // cell Morton index in a block -> cx | cy << 8
     uint8_t cnt[256];
 };
+
+// The block a warp is working in: its key-space origin and, for the column
+// layout, the lattice cell of its first key (every cell of such a block lies
+// in the same slice tile).
+struct WarpBlock {
+    uint32_t b, base, count;
+    uint32_t X0, Y0;
+    int ox, oy, oz;
+    bool have;
+};
+
+__device__ __forceinline__ uint32_t compact32(uint32_t v) {
+    v &= 0x55555555u;
+    v = (v | (v >> 1)) & 0x33333333u;
+    v = (v | (v >> 2)) & 0x0f0f0f0fu;
+    v = (v | (v >> 4)) & 0x00ff00ffu;
+    v = (v | (v >> 8)) & 0x0000ffffu;
+    return v;
+}
 
 __device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         S.cnt[i] = c_vertex_count_t[i];
         S.edge[i] = c_edge_nibbles[i];
+    }
+    for (int i = threadIdx.x; i < kBlockKeys; i += blockDim.x) {
+        int cx, cy;
+        morton10((uint32_t)i, cx, cy);
+        S.morton[i] = (uint16_t)(cx | (cy << 8));
     }
     for (int i = threadIdx.x; i < V.top_cached; i += blockDim.x) S.top[i] = V.levels[i];
     __syncthreads();
@@ -116,8 +141,8 @@ struct VertexCell {
     int k;
 };
 
-__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp, uint32_t b,
-                                                uint32_t key) {
+__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp,
+                                                const WarpBlock& B, uint32_t key) {
     const uint16_t* pref = S.pref[warp];
     int lo = 0;
 #pragma unroll
@@ -127,30 +152,47 @@ __device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseS
     r.code = (S.codew[warp][lo >> 2] >> (8 * (lo & 3))) & 0xff;
     r.k = (int)key - ((int)pref[lo] - (int)S.cnt[r.code]);
     r.k = min(max(r.k, 0), 15);  // in range whenever key < block count (table reads stay in bounds)
-    int cx, cy;
-    morton10((uint32_t)lo, cx, cy);
-    const uint32_t X = (morton_compact(b) << 5) + (uint32_t)cx;
-    const uint32_t Y = (morton_compact((uint64_t)b >> 1) << 5) + (uint32_t)cy;
-    virtual_to_cell(V, X, Y, r.x, r.y, r.z);
+    const uint32_t m = S.morton[lo];
+    const int cx = (int)(m & 0xffu), cy = (int)(m >> 8);
+    if (V.column_layout) {
+        r.x = B.ox + cx;
+        r.y = B.oy + cy;
+        r.z = B.oz;
+    } else {
+        virtual_to_cell(V, B.X0 + (uint32_t)cx, B.Y0 + (uint32_t)cy, r.x, r.y, r.z);
+    }
     return r;
 }
 
 // Steps 1-2 for one round of 32 vertices of a warp; returns false for lanes
-// without a vertex.  (bb, bbase, bcount) is the warp's cached block.
+// without a vertex.  B is the warp's cached block.
+__device__ __forceinline__ void enter_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t key,
+                                            WarpBlock& B) {
+    descend(V, S, key, B.b, B.base, B.count);  // uniform across the warp
+    load_block(V, S, warp, lane, B.b);
+    B.X0 = compact32(B.b) << 5;
+    B.Y0 = compact32(B.b >> 1) << 5;
+    virtual_to_cell(V, B.X0, B.Y0, B.ox, B.oy, B.oz);
+    B.have = true;
+}
+
 __device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t v,
-                                               bool act, uint32_t& bb, uint32_t& bbase, uint32_t& bcount,
-                                               bool& have, VertexCell& out) {
-    unsigned int pending = __ballot_sync(0xffffffffu, act);
+                                               bool act, WarpBlock& B, VertexCell& out) {
+    const unsigned int actm = __ballot_sync(0xffffffffu, act);
+    // common case: the whole round lies in the cached block
+    const uint32_t vfirst = __shfl_sync(0xffffffffu, v, __ffs(actm) - 1);
+    const uint32_t vlast = __shfl_sync(0xffffffffu, v, 31 - __clz(actm));
+    if (B.have && vfirst >= B.base && vlast - B.base < B.count) {
+        if (act) out = find_cell(V, S, warp, B, v - B.base);
+        return act;
+    }
+    unsigned int pending = actm;
     while (pending) {
         const int leader = __ffs(pending) - 1;
         const uint32_t vl = __shfl_sync(0xffffffffu, v, leader);
-        if (!have || vl < bbase || vl - bbase >= bcount) {
-            descend(V, S, vl, bb, bbase, bcount);  // uniform across the warp
-            load_block(V, S, warp, lane, bb);
-            have = true;
-        }
-        const bool mine = ((pending >> lane) & 1u) && v >= bbase && v - bbase < bcount;
-        if (mine) out = find_cell(V, S, warp, bb, v - bbase);
+        if (!B.have || vl < B.base || vl - B.base >= B.count) enter_block(V, S, warp, lane, vl, B);
+        const bool mine = ((pending >> lane) & 1u) && v >= B.base && v - B.base < B.count;
+        if (mine) out = find_cell(V, S, warp, B, v - B.base);
         pending &= ~__ballot_sync(0xffffffffu, mine);
         __syncwarp();
     }
@@ -162,6 +204,27 @@ struct EdgeGeom {
     int axis;
     int edge;
 };
+
+// Dynamic work queue over vertex chunks (balances the persistent grid):
+// lane 0 takes the next chunk for its warp.
+__device__ __forceinline__ uint32_t next_chunk(const Volume& V, int lane) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&V.ctrl->work_next, 1u);
+    return __shfl_sync(0xffffffffu, c, 0);
+}
+
+// The last CTA to finish resets the queue for the next launch on the stream.
+__device__ __forceinline__ void finish_queue(const Volume& V) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&V.ctrl->work_done, 1u) == gridDim.x - 1) {
+            V.ctrl->work_next = 0;
+            V.ctrl->work_done = 0;
+            __threadfence();
+        }
+    }
+}
 
 __device__ __forceinline__ EdgeGeom edge_of(const TraverseSmem& S, const VertexCell& c) {
     EdgeGeom g;
@@ -191,16 +254,16 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
     }
     constexpr uint32_t VW = 32u * kTraverseRounds;
     const uint32_t nchunks = (N + VW - 1) / VW;
-    uint32_t bb = 0, bbase = 0, bcount = 0;
-    bool have = false;
-    for (uint32_t chunk = blockIdx.x * kWarps + warp; chunk < nchunks; chunk += gridDim.x * kWarps) {
+    WarpBlock B;
+    B.have = false;
+    for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
         for (int r = 0; r < kTraverseRounds; r++) {
             const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
             VertexCell c;
-            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, have, c)) continue;
+            if (!resolve_vertex(V, S, warp, lane, v, act, B, c)) continue;
             const EdgeGeom g = edge_of(S, c);
             float p[3], n[3], t;
             edge_vertex<FT, MODE>(V, g.a, g.axis, c.x, c.y, c.z, g_binary_normals + 3 * (16 * c.code + c.k), p, n,
@@ -218,6 +281,7 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
             if (O.dbg_t) O.dbg_t[o] = t;
         }
     }
+    finish_queue(V);
 }
 
 // ---------------------------------------------------------------------------
@@ -250,26 +314,27 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
     const float iso = V.iso;
     constexpr uint32_t VW = 32u * kTraverseRounds;
     const uint32_t nchunks = (N + VW - 1) / VW;
-    uint32_t bb = 0, bbase = 0, bcount = 0;
-    bool have = false;
-    for (uint32_t chunk = blockIdx.x * kWarps + warp; chunk < nchunks; chunk += gridDim.x * kWarps) {
+    WarpBlock B;
+    B.have = false;
+    for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
         for (int r = 0; r < kTraverseRounds; r++) {
             const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
             VertexCell c;
-            if (!resolve_vertex(V, S, warp, lane, v, act, bb, bbase, bcount, have, c)) continue;
+            if (!resolve_vertex(V, S, warp, lane, v, act, B, c)) continue;
             const EdgeGeom g = edge_of(S, c);
             const int ax = g.axis;
             const int ex = ax == 0, ey = ax == 1, ez = ax == 2;
-            const EdgeSamples<FT> f(V, g.a, ax, c.x, c.y, c.z);
+            EdgeField F;
+            gather_edge<FT, MODE == kModeCentral>(V, g.a, ax, c.x, c.y, c.z, F);
             const unsigned long long o = V.vertex_base + v;
             const float4 dp = A.dpos ? __ldg(A.dpos + o) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 dn = A.dnrm ? __ldg(A.dnrm + o) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float dpv[3] = {dp.x, dp.y, dp.z};
             const float dnv[3] = {dn.x * V.scale[0], dn.y * V.scale[1], dn.z * V.scale[2]};
-            const float va = f.fa(), vb = f.fb();
+            const float va = F.va, vb = F.vb;
             const float den = va - vb;
             const FF tf = ff_ratio_of_diffs(va, iso, va, vb);
             const float t = tf.hi + tf.lo;
@@ -279,16 +344,16 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 const int dx = i == 0, dy = i == 1, dz = i == 2;
-                const float fa_p = (i == ax) ? vb : f.fa_plus(i);
-                const float fb_p = f.fb_plus(i);
+                const float fa_p = F.ap[i];
+                const float fb_p = F.bp[i];
                 if (MODE == kModeForward) {
                     dLdt += dnv[i] * (fa_p - fb_p);
                     const float wa = -omt * dnv[i], wb = -t * dnv[i];
                     if (i == ax) gb += wa; else scatter(V, A.dfield, g.a, dx, dy, dz, wa);
                     scatter(V, A.dfield, g.a, ex + dx, ey + dy, ez + dz, wb);
                 } else {
-                    const float fa_m = f.fa_minus(i);
-                    const float fb_m = (i == ax) ? va : f.fb_minus(i);
+                    const float fa_m = F.am[i];
+                    const float fb_m = F.bm[i];
                     dLdt += -0.5f * dnv[i] * ((fb_p - fb_m) - (fa_p - fa_m));
                     const float wa = -0.5f * omt * dnv[i], wb = -0.5f * t * dnv[i];
                     if (i == ax) gb += wa; else scatter(V, A.dfield, g.a, dx, dy, dz, wa);
@@ -304,6 +369,7 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
             scatter(V, A.dfield, g.a, ex, ey, ez, gb);
         }
     }
+    finish_queue(V);
 }
 
 // ---------------------------------------------------------------------------
