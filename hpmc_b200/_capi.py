@@ -28,6 +28,8 @@ ERR_BROKEN = 9
 ERR_NO_FIELD = 10
 ERR_OVERFLOW = 11
 ERR_TIMEOUT = 12
+ERR_TOO_LARGE = 13
+STATIC_SCRATCH_BYTES = 4 << 20
 
 STATUS_NAMES = {v: k for k, v in globals().items() if k.startswith("ERR_") or k == "OK"}
 
@@ -80,6 +82,8 @@ _SIGS = {
     "HPMCsetTraversalDebugBuffers": (C.c_int, [vp, vp, vp]),
     "HPMCgetDeviceStatus": (C.c_int, [vp, C.POINTER(C.c_uint)]),
     "HPMCgetClassifyPath": (C.c_int, [vp, C.POINTER(C.c_int)]),
+    "HPMCextractStatic": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_float,
+                                    C.c_int, C.POINTER(C.c_float), vp, vp, C.c_size_t, vp, vp]),
 }
 
 _lib = None

@@ -786,3 +786,201 @@ int HPMCgetDeviceStatus(HPMCHistoPyramid* h, unsigned int* status) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// HPMCextractStatic: build + count + extract with every scratch buffer in one
+// fixed device array (no device allocation).  See include/hpmc.h.
+// ============================================================================
+namespace {
+
+// The scratch of HPMCextractStatic.  In host code `g_static_scratch` names a
+// host-side stand-in, not device memory: kernels are given the address that
+// cudaGetSymbolAddress returns for the current device.
+static __device__ __align__(256) unsigned char g_static_scratch[HPMC_STATIC_SCRATCH_BYTES];
+
+constexpr int kStaticMaxDevices = 64;
+
+struct StaticDeviceState {
+    unsigned char* scratch = nullptr;  // device address of g_static_scratch on this device
+    int num_sms = 0;
+    int traverse_ctas_per_sm = 0;
+    bool ready = false;
+};
+
+std::mutex g_static_mu;
+StaticDeviceState g_static_dev[kStaticMaxDevices];
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+// Once per device, with that device current: look up the scratch array's
+// device address and configure the kernels.
+int static_device_setup(StaticDeviceState** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return HPMC_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kStaticMaxDevices) return HPMC_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    StaticDeviceState& s = g_static_dev[dev];
+    if (!s.ready) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_static_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return HPMC_ERR_CUDA;
+        }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return HPMC_ERR_CUDA;
+        }
+        s.scratch = static_cast<unsigned char*>(p);
+        s.num_sms = prop.multiProcessorCount;
+        s.traverse_ctas_per_sm = hpmc::traverse_blocks_per_sm();
+        hpmc::column_smem_ok();
+        s.ready = true;
+    }
+    *out = &s;
+    return HPMC_OK;
+}
+
+}  // namespace
+
+extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_size, GLsizei y_size,
+                                 GLsizei z_size, size_t row_pitch_bytes, size_t slice_pitch_bytes, GLfloat iso,
+                                 int normal_mode, const GLfloat* extent, float* positions, float* normals,
+                                 size_t capacity_vertices, unsigned int* device_vertex_count,
+                                 void* cuda_stream) {
+    if (!field || !device_vertex_count || scalar_type < HPMC_SCALAR_F32 || scalar_type > HPMC_SCALAR_UNORM8 ||
+        (normal_mode != HPMC_NORMALS_FORWARD && normal_mode != HPMC_NORMALS_CENTRAL) ||
+        (positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16))
+        return HPMC_ERR_INVALID_VALUE;
+    const int lattice[3] = {x_size, y_size, z_size};
+    const int cells[3] = {x_size - 1, y_size - 1, z_size - 1};
+    int L[6];
+    if (!determine_layout(lattice, cells, L)) return HPMC_ERR_LAYOUT;  // init.cpp:82-103
+    StaticDeviceState* dev = nullptr;
+    int st = static_device_setup(&dev);
+    if (st != HPMC_OK) return st;
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+
+    Volume V{};
+    for (int i = 0; i < 3; i++) {
+        V.lattice[i] = lattice[i];
+        V.cells[i] = cells[i];
+        const float e = extent ? extent[i] : 1.0f;
+        V.scale[i] = e / (float)cells[i];
+        V.dscale[i] = (double)e / (double)cells[i];
+    }
+    V.tile_x = L[0];
+    V.tile_y = L[1];
+    V.layout_x = L[2];
+    V.layout_y = L[3];
+    V.size_l2 = L[4];
+    auto ilog2 = [](int v) {
+        int e = 0;
+        while ((1 << e) < v) e++;
+        return e;
+    };
+    V.wx_l2 = ilog2(2 * L[0]);
+    V.wy_l2 = ilog2(2 * L[1]);
+    V.lx_l2 = ilog2(L[2]);
+    V.jtop = std::max(hpmc::kBlockLevel, V.size_l2 + 1);
+    long long off = 0;
+    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
+        V.level_off[j] = off;
+        off += (hpmc::level_entries(V.size_l2, j) + 3) & ~3ll;
+    }
+    const long long level_entries_total = off;
+    V.nblocks = hpmc::level_entries(V.size_l2, hpmc::kBlockLevel);
+    V.top_cached = 0;
+    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
+        const long long end = V.level_off[j] + ((hpmc::level_entries(V.size_l2, j) + 3) & ~3ll);
+        if (end > hpmc::kTopCacheEntries) break;
+        V.top_cached = (int)end;
+    }
+    V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
+    V.nfx = (V.cells[0] + 31) / 32;
+    V.nfy = (V.cells[1] + 31) / 32;
+    V.column_slices = hpmc::kColumnSliceChoices[3];
+    for (int zc : hpmc::kColumnSliceChoices) {
+        if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= 12ll * dev->num_sms) {
+            V.column_slices = zc;
+            break;
+        }
+    }
+    const long long slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
+
+    // carve the scratch: control block | dense levels | code arena
+    const size_t ctrl_bytes = align256(sizeof(Ctrl));
+    const size_t levels_bytes = align256(sizeof(uint32_t) * (size_t)level_entries_total);
+    const size_t arena_bytes = sizeof(uint32_t) * hpmc::kBlockWords * (size_t)slots;
+    if (ctrl_bytes + levels_bytes + arena_bytes > (size_t)HPMC_STATIC_SCRATCH_BYTES) return HPMC_ERR_TOO_LARGE;
+    unsigned char* base = dev->scratch;
+    V.ctrl = reinterpret_cast<Ctrl*>(base);
+    V.levels = reinterpret_cast<uint32_t*>(base + ctrl_bytes);
+    V.arena = reinterpret_cast<uint32_t*>(base + ctrl_bytes + levels_bytes);
+    V.arena_slots = slots;
+
+    // field
+    const size_t es = elem_size(scalar_type);
+    const size_t rp = row_pitch_bytes ? row_pitch_bytes : (size_t)lattice[0] * es;
+    const size_t sp = slice_pitch_bytes ? slice_pitch_bytes : rp * (size_t)lattice[1];
+    if (rp % es || sp % es || rp < (size_t)lattice[0] * es || sp < rp * (size_t)lattice[1])
+        return HPMC_ERR_INVALID_VALUE;
+    V.field = field;
+    V.ftype = scalar_type == HPMC_SCALAR_F32 ? hpmc::kFieldF32
+              : scalar_type == HPMC_SCALAR_U8 ? hpmc::kFieldU8
+                                              : hpmc::kFieldUNorm8;
+    V.row_pitch = (long long)(rp / es);
+    V.slice_pitch = (long long)(sp / es);
+    V.idx32 = (V.slice_pitch * ((long long)lattice[2] + 1) < (1ll << 31)) ? 1 : 0;
+    V.iso = iso;
+    V.binary = 0;
+    {
+        int n = 0;
+        for (int b = 0; b < 256; b++) {
+            const float f = (V.ftype == hpmc::kFieldUNorm8) ? (float)b / 255.0f : (float)b;
+            if (f < iso) n = b + 1;
+        }
+        V.u8_thr = n;
+    }
+    CUtensorMap tmap;
+    bool have_tmap = false;
+    if (V.column_layout && ((uintptr_t)field % 16 == 0) && rp % 16 == 0 && sp % 16 == 0) {
+        auto enc = tensor_map_encoder();
+        if (enc) {
+            const cuuint64_t dims[3] = {(cuuint64_t)lattice[0], (cuuint64_t)lattice[1], (cuuint64_t)lattice[2]};
+            const cuuint64_t strides[2] = {(cuuint64_t)rp, (cuuint64_t)sp};
+            const bool f32 = scalar_type == HPMC_SCALAR_F32;
+            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, (cuuint32_t)hpmc::kLayersPerBox};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            have_tmap = enc(&tmap, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
+                            const_cast<void*>(field), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+    }
+
+    // the array keeps the previous call's contents: clear the control block
+    // (counters, status) and the dense levels (padding entries read as zero)
+    cudaError_t e = cudaMemsetAsync(base, 0, ctrl_bytes + levels_bytes, stream);
+    if (e == cudaSuccess) e = hpmc::launch_classify(V, have_tmap ? &tmap : nullptr, dev->num_sms * 16, stream);
+    if (e == cudaSuccess) e = hpmc::launch_reduce(V, stream);
+    if (e == cudaSuccess) {
+        hpmc::TraverseOut O{};
+        O.pos = reinterpret_cast<float4*>(positions);
+        O.nrm = reinterpret_cast<float4*>(normals);
+        O.capacity = capacity_vertices;
+        e = hpmc::launch_traverse(V, O, normal_mode, dev->num_sms * dev->traverse_ctas_per_sm, stream);
+    }
+    // full vertex count (little-endian low word of the 64-bit total)
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(device_vertex_count, &V.ctrl->total, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                            stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return HPMC_ERR_CUDA;
+    }
+    return HPMC_OK;
+}

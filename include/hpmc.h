@@ -49,7 +49,8 @@ typedef enum HPMCStatus {
     HPMC_ERR_BROKEN = 9,          /* handle is broken until reconfigured */
     HPMC_ERR_NO_FIELD = 10,       /* no field source set */
     HPMC_ERR_OVERFLOW = 11,       /* vertex count does not fit 32 bits */
-    HPMC_ERR_TIMEOUT = 12         /* a bounded device wait gave up */
+    HPMC_ERR_TIMEOUT = 12,        /* a bounded device wait gave up */
+    HPMC_ERR_TOO_LARGE = 13       /* lattice needs more than the fixed scratch of HPMCextractStatic */
 } HPMCStatus;
 
 /* ---- field element types of device arrays ---- */
@@ -241,6 +242,37 @@ int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
  * cell block inside one slice tile, 16-byte aligned array field), 0 = generic
  * per-block kernel (narrow tiles, unaligned pitches, functor fields). */
 int HPMCgetClassifyPath(struct HPMCHistoPyramid* h, int* path);
+
+/* ---- extraction without device allocation ----
+ *
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory at extraction time: hosts that reserve the whole GPU memory budget
+ * up front (render engines and plugins handed fixed buffers) and real-time
+ * loops where cudaMalloc/cudaFree -- which synchronise the device -- are not
+ * allowed.  One call builds, counts and extracts like HPMCbuildHistopyramid +
+ * HPMCextractVerticesToBuffers, but every scratch buffer (pyramid levels,
+ * code arena, control block) lives in one fixed device array of
+ * HPMC_STATIC_SCRATCH_BYTES that the library holds on every GPU that loads
+ * it until the process exits; it calls no cudaMalloc, cudaFree or other
+ * allocating routine.
+ *
+ * The caller passes the field (device pointer, pitches in bytes, 0 = dense),
+ * the outputs (float4 positions and normals, either may be NULL; capacity
+ * in vertices) and a device uint32 that receives the full vertex count (so
+ * that count > capacity shows truncation).  extent may be NULL (1,1,1).
+ * Work is issued on `cuda_stream`.  Lattices whose pyramid and code arena do
+ * not fit the scratch (e.g. larger than about 160^3) are rejected with
+ * HPMC_ERR_TOO_LARGE.  The first call on a device looks up the scratch
+ * array's device address and configures the kernels, so make it before any
+ * stream capture.  All calls share the one scratch array, which keeps the
+ * last call's contents (the call clears what must start at zero): calls that
+ * overlap on the GPU -- different streams, or concurrent host threads -- race
+ * and must be serialised by the caller. */
+#define HPMC_STATIC_SCRATCH_BYTES (4u << 20)
+int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_size, GLsizei y_size, GLsizei z_size,
+                      size_t row_pitch_bytes, size_t slice_pitch_bytes, GLfloat iso, int normal_mode,
+                      const GLfloat* extent, float* positions, float* normals, size_t capacity_vertices,
+                      unsigned int* device_vertex_count, void* cuda_stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop
