@@ -39,6 +39,12 @@ WORKLOAD = ("cayley_512: FP32 512^3 lattice, Cayley cubic 16xyz+4(x^2+y^2+z^2)-1
             "iso 0, central-difference normals, float4 position+normal streams")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) of one build (classify_column_tma + reduce_levels)
+# per field byte, from ncu captures on the 384^3 Cayley field
+# (profiles/classify_column_tma_cayley384.txt, profiles/reduce_levels_cayley384.txt):
+# (226,523,136 + 11,095,296 + 1,067,264) / 226,492,416.  Traffic grows with
+# the field, so the 512^3 figure is this ratio times the field bytes.
+BUILD_TRAFFIC_PER_FIELD_BYTE = (226523136 + 11095296 + 1067264) / 226492416
 
 
 def hbm_peak():
@@ -162,6 +168,90 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, dev, stream):
+    """64 uneven FP32 metaball volumes: one CUDA-graph replay of the batched
+    extractor vs the plain per-volume loop through the handle API (build,
+    acquire count, extract), both on the same stream, CUDA events."""
+    import torch
+
+    import hpmc_b200 as H
+    from hpmc_b200 import datasets
+
+    vols = datasets.batch_64()
+    tensors = [torch.from_numpy(f).to(dev) for f, _ in vols]
+    isos = [iso for _, iso in vols]
+    cells = sum((f.shape[0] - 1) * (f.shape[1] - 1) * (f.shape[2] - 1) for f, _ in vols)
+    field_bytes = sum(f.nbytes for f, _ in vols)
+    C = H.default_constants()
+    # plain loop: one handle per volume, created and sized outside the timed region
+    hps, ths, outs = [], [], []
+    with torch.cuda.stream(stream):
+        for t, iso in zip(tensors, isos):
+            hp = H.HistoPyramid(C)
+            hp.set_stream(stream)
+            hp.set_field_device(t)
+            hp.set_normal_mode(H.NORMALS_CENTRAL)
+            hp.build(iso)
+            n = hp.acquire_number_of_vertices()
+            th = H.TraversalHandle(hp)
+            pos = torch.empty((max(n, 1), 4), dtype=torch.float32, device=dev)
+            nrm = torch.empty_like(pos)
+            th.set_buffers(pos, nrm, n)
+            hps.append(hp)
+            ths.append(th)
+            outs.append(n)
+    total = sum(outs)
+
+    def plain():
+        for hp, th, iso in zip(hps, ths, isos):
+            hp.build(iso)
+            hp.acquire_number_of_vertices()
+            th.extract()
+
+    steps = max(3, min(args.steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            plain()
+        stream.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            plain()
+        e1.record(stream)
+        stream.synchronize()
+    plain_ms = e0.elapsed_time(e1) / steps
+
+    b = H.Batch(tensors, isos, normals=H.NORMALS_CENTRAL)
+    pos = torch.empty((total, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty_like(pos)
+    with torch.cuda.stream(stream):
+        tuning = b.autotune(pos, nrm, total, stream=stream)
+        for _ in range(3):
+            b.extract(pos, nrm, total, stream=stream)
+        stream.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            b.extract(pos, nrm, total, stream=stream)
+        e1.record(stream)
+        stream.synchronize()
+    batched_ms = e0.elapsed_time(e1) / steps
+    offs = b.offsets()
+    assert offs[-1] == total, (offs[-1], total)
+    for th in ths:
+        th.close()
+    for hp in hps:
+        hp.close()
+    b.close()
+    return {"workload": "batch_64: 64 FP32 volumes, edges log-uniform [32,192] (x4), 4-32 metaballs, iso U[0.8,1.5], "
+                        "central normals",
+            "volumes": len(vols), "cells": cells, "field_bytes": field_bytes, "vertices": total,
+            "plain_ms": plain_ms, "batched_ms": batched_ms,
+            "plain_vols_per_s": len(vols) / (plain_ms * 1e-3), "batched_vols_per_s": len(vols) / (batched_ms * 1e-3),
+            "speedup": plain_ms / batched_ms, "batched_gcells_per_s": cells / (batched_ms * 1e-3) / 1e9,
+            "tuning": {"column_slices": tuning[0], "traverse_ctas_per_sm": tuning[1], "rounds": tuning[2]},
+            "graph": True, "steps": steps}
+
+
 def run_hpmc(args, rank, world, local_rank):
     import torch
 
@@ -239,7 +329,9 @@ def run_hpmc(args, rank, world, local_rank):
     alg_bytes = field_bytes + out_bytes
     roof = {"kernel": "build = classify_column_tma + reduce_levels (classify dominates)",
             "bound": "hbm", "achieved": field_bytes / (build_avg * 1e-3) / 1e9, "peak": peak,
-            "unit": "GB/s", "frac": field_bytes / (build_avg * 1e-3) / 1e9 / peak, "traffic": None,
+            "unit": "GB/s", "frac": field_bytes / (build_avg * 1e-3) / 1e9 / peak,
+            "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes,
+            "traffic_source": "ncu dram__bytes_read+write of the 384^3 capture, scaled by field bytes",
             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": field_bytes,
             "avg_launch_ms": build_avg}
     step_frac = alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak
@@ -277,6 +369,10 @@ def run_hpmc(args, rank, world, local_rank):
         e2e = {"value": cells / (e2e_ms * 1e-3) / 1e9, "unit": "Gcells/s", "h2d_bytes_per_step": field_bytes,
                "d2h_bytes_per_step": 32 * nverts, "ms_per_step": e2e_ms}
 
+    batched = None
+    if not args.no_batch:
+        batched = run_batched(args, dev, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(field_np, iso)
@@ -297,6 +393,7 @@ def run_hpmc(args, rank, world, local_rank):
                 "vertices_per_s": nverts * world * args.steps / (total_ms * 1e-3),
                 "build_ms": build_avg, "traverse_ms": trav_avg,
                 "cpu_baseline": cpu, "e2e": e2e,
+                "batched": batched,
                 "gpu_launches": 3 * args.steps,
                 "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
@@ -313,6 +410,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--lattice", type=int, default=512, help="lattice edge (profiling runs use smaller ones)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-extraction leg")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

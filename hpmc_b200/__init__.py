@@ -18,7 +18,7 @@ from ._capi import (NORMALS_CENTRAL, NORMALS_FORWARD, SCALAR_F32, SCALAR_U8,  # 
                     SCALAR_UNORM8, STATUS_NAMES)
 
 __all__ = [
-    "Constants", "HistoPyramid", "TraversalHandle", "HPMCError", "extract", "lib",
+    "Constants", "HistoPyramid", "TraversalHandle", "Batch", "HPMCError", "extract", "lib",
     "NORMALS_FORWARD", "NORMALS_CENTRAL", "SCALAR_F32", "SCALAR_U8", "SCALAR_UNORM8",
 ]
 
@@ -237,6 +237,89 @@ class TraversalHandle:
     def close(self):
         if self.ptr:
             lib().HPMCdestroyTraversalHandle(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched extraction (HPMCcreateBatch ... HPMCbatchExtract): many (z, y, x)
+    CUDA fields of one dtype, uneven sizes and per-volume iso-values, extracted by
+    one CUDA-graph replay.  Volume v's vertices are rows offsets[v]:offsets[v+1]."""
+
+    def __init__(self, fields, isos, *, extents=None, normals: int = NORMALS_FORWARD, unorm: bool = False,
+                 constants: Constants | None = None):
+        self.constants = constants or default_constants()
+        self.fields = list(fields)
+        n = len(self.fields)
+        vols = (_capi.BatchVolume * n)()
+        for i, (f, iso) in enumerate(zip(self.fields, isos)):
+            if not f.is_cuda or f.stride(2) != 1:
+                raise ValueError("fields must be CUDA tensors with unit stride along x")
+            es = f.element_size()
+            fz, fy, fx = f.shape
+            vols[i].field = f.data_ptr()
+            vols[i].scalar_type = _scalar_type(f, unorm)
+            vols[i].size[:] = [fx, fy, fz]
+            vols[i].row_pitch_bytes = f.stride(1) * es
+            vols[i].slice_pitch_bytes = f.stride(0) * es
+            vols[i].iso = float(iso)
+            ext = extents[i] if extents is not None else (1.0, 1.0, 1.0)
+            vols[i].extent[:] = [float(e) for e in ext]
+        self.count = n
+        self.ptr = C.c_void_p()
+        _check(lib().HPMCcreateBatch(self.constants.ptr, C.cast(vols, C.c_void_p), n, C.byref(self.ptr)),
+               "HPMCcreateBatch")
+        self.set_normal_mode(normals)
+
+    def set_normal_mode(self, mode: int):
+        _check(lib().HPMCbatchSetNormalMode(self.ptr, int(mode)), "HPMCbatchSetNormalMode")
+
+    def set_iso_values(self, isos):
+        buf = (C.c_float * self.count)(*[float(v) for v in isos])
+        _check(lib().HPMCbatchSetIsoValues(self.ptr, buf), "HPMCbatchSetIsoValues")
+
+    def set_tuning(self, column_slices: int = 0, traverse_ctas_per_sm: int = 0, rounds: int = 0):
+        _check(lib().HPMCbatchSetTuning(self.ptr, column_slices, traverse_ctas_per_sm, rounds), "HPMCbatchSetTuning")
+
+    def tuning(self):
+        out = (C.c_int * 3)()
+        _check(lib().HPMCbatchGetTuning(self.ptr, out), "HPMCbatchGetTuning")
+        return tuple(out)
+
+    def extract(self, pos, nrm, capacity: int | None = None, stream=None):
+        """Asynchronous: build, count and extract every volume into pos/nrm (float4 rows)."""
+        import torch
+
+        cap = capacity if capacity is not None else (pos if pos is not None else nrm).shape[0]
+        st = stream if stream is not None else torch.cuda.current_stream()
+        _check(lib().HPMCbatchExtract(self.ptr, _ptr(pos), _ptr(nrm), int(cap), st.cuda_stream), "HPMCbatchExtract")
+
+    def offsets(self, allow_truncation: bool = False):
+        """count + 1 output offsets of the last extraction (waits for it)."""
+        out = (C.c_ulonglong * (self.count + 1))()
+        st = lib().HPMCbatchGetOffsets(self.ptr, out)
+        if st != _capi.OK and not (allow_truncation and st == _capi.ERR_CAPACITY):
+            raise HPMCError(st, "HPMCbatchGetOffsets")
+        return [int(v) for v in out]
+
+    def autotune(self, pos, nrm, capacity: int | None = None, stream=None):
+        import torch
+
+        cap = capacity if capacity is not None else (pos if pos is not None else nrm).shape[0]
+        st = stream if stream is not None else torch.cuda.current_stream()
+        out = (C.c_int * 3)()
+        _check(lib().HPMCbatchAutotune(self.ptr, _ptr(pos), _ptr(nrm), int(cap), st.cuda_stream, out),
+               "HPMCbatchAutotune")
+        return tuple(out)
+
+    def close(self):
+        if self.ptr:
+            lib().HPMCdestroyBatch(self.ptr)
             self.ptr = None
 
     def __del__(self):

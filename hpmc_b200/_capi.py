@@ -84,7 +84,32 @@ _SIGS = {
     "HPMCgetClassifyPath": (C.c_int, [vp, C.POINTER(C.c_int)]),
     "HPMCextractStatic": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_float,
                                     C.c_int, C.POINTER(C.c_float), vp, vp, C.c_size_t, vp, vp]),
+    # batched extraction
+    "HPMCcreateBatch": (C.c_int, [vp, vp, C.c_int, C.POINTER(vp)]),
+    "HPMCdestroyBatch": (None, [vp]),
+    "HPMCbatchSetIsoValues": (C.c_int, [vp, C.POINTER(C.c_float)]),
+    "HPMCbatchSetNormalMode": (C.c_int, [vp, C.c_int]),
+    "HPMCbatchExtract": (C.c_int, [vp, vp, vp, C.c_size_t, vp]),
+    "HPMCbatchGetOffsets": (C.c_int, [vp, C.POINTER(C.c_ulonglong)]),
+    "HPMCbatchGetDeviceOffsets": (C.c_int, [vp, C.POINTER(vp)]),
+    "HPMCbatchSetTuning": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+    "HPMCbatchGetTuning": (C.c_int, [vp, C.POINTER(C.c_int)]),
+    "HPMCbatchAutotune": (C.c_int, [vp, vp, vp, C.c_size_t, vp, C.POINTER(C.c_int)]),
 }
+
+
+class BatchVolume(C.Structure):
+    """HPMCBatchVolume (include/hpmc.h)."""
+
+    _fields_ = [
+        ("field", C.c_void_p),
+        ("scalar_type", C.c_int),
+        ("size", C.c_int * 3),
+        ("row_pitch_bytes", C.c_size_t),
+        ("slice_pitch_bytes", C.c_size_t),
+        ("iso", C.c_float),
+        ("extent", C.c_float * 3),
+    ]
 
 _lib = None
 

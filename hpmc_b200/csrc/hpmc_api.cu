@@ -21,6 +21,7 @@
 
 #include "hpmc.h"
 #include "hpmc_device.cuh"
+#include "hpmc_host.h"
 #include "hpmc_kernels.h"
 
 using hpmc::Ctrl;
@@ -28,7 +29,7 @@ using hpmc::Volume;
 
 namespace {
 
-constexpr uint32_t kMagicConstants = 0x48504331u;  // "HPC1"
+using hpmc::host::kMagicConstants;
 constexpr uint32_t kMagicPyramid = 0x48505931u;
 constexpr uint32_t kMagicTraversal = 0x48505431u;
 
@@ -44,60 +45,11 @@ std::mutex g_fields_mu;
 std::map<GLuint, FieldDesc> g_fields;
 GLuint g_next_field = 1;
 
-// ---------------------------------------------------------------------------
-// init.cpp:72-149 -- layout of the tiled base level.  For a 1-cell axis the
-// reference shifts by -1 (undefined); the exponent is clamped at 0 here.
-bool determine_layout(const int lattice[3], const int cells[3], int out[6]) {
-    for (int i = 0; i < 3; i++) {
-        if (lattice[i] < 2 || lattice[i] > 16384) return false;  // init.cpp:82-90
-        if (lattice[i] <= cells[i]) return false;                // init.cpp:98-103
-        if (cells[i] < 1) return false;
-    }
-    auto tile_exp = [](int c) {
-        int e = (int)ceilf(log2f(static_cast<float>(c) / 2.0f));  // init.cpp:106-111
-        return e < 0 ? 0 : e;
-    };
-    const int tx = 1 << tile_exp(cells[0]);
-    const int ty = 1 << tile_exp(cells[1]);
-    const float aspect = static_cast<float>(tx) / static_cast<float>(ty);
-    const float lxe = std::max(0.0f, ceilf(log2f(sqrtf(static_cast<float>(cells[2]) / aspect))));
-    const int lx = 1 << static_cast<int>(lxe);                     // init.cpp:116-119
-    const int ly = (cells[2] + lx - 1) / lx;                       // init.cpp:120-121
-    const int l2 = static_cast<int>(ceilf(log2f(static_cast<float>(std::max(tx * lx, ty * ly)))));
-    const int size = 1 << l2;                                      // init.cpp:123-128
-    out[0] = tx;
-    out[1] = ty;
-    out[2] = size / tx;                                            // init.cpp:129-130
-    out[3] = size / ty;
-    out[4] = l2;
-    out[5] = size;
-    return true;
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-size_t elem_size(int type) { return type == HPMC_SCALAR_F32 ? 4 : 1; }
+using hpmc::host::determine_layout;  // init.cpp:72-149
+using hpmc::host::elem_size;
+using hpmc::host::tensor_map_encoder;
 
 }  // namespace
-
-struct HPMCConstants {
-    uint32_t magic;
-    int device;
-    int num_sms;
-    int traverse_ctas_per_sm;
-};
 
 struct HPMCHistoPyramid {
     uint32_t magic = kMagicPyramid;

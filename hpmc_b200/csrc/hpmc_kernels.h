@@ -27,7 +27,35 @@ struct AdjointIO {
     unsigned long long count;      // vertices to differentiate (<= vertex count)
 };
 
+// Batch-wide control block (device).
+struct BatchCtrl {
+    unsigned int reduce_done;     // volumes whose pyramid is complete (the last one scans)
+    unsigned int work_next;       // traversal work queue: next item to hand out
+    unsigned int work_done;       // traversal CTAs finished (the last one resets the queue)
+    unsigned int status;          // sticky kStatus* bits of the batch
+    unsigned long long total;     // vertices of all volumes
+};
+
+// Kernel view of a batch (all arrays in device memory).
+struct BatchDev {
+    const Volume* vols;            // per-volume descriptors (top_cached = 0)
+    const CUtensorMap* tmaps;      // per-volume column tensor maps (64-byte aligned)
+    const uint32_t* brick_start;   // nvol + 1: column bricks before volume v
+    const uint32_t* reduce_start;  // nvol + 1: reduction chunks before volume v
+    unsigned long long* vbase;     // nvol + 1: first output vertex of volume v (written by the reduction)
+    uint32_t* chunk_start;         // nvol + 1: traversal work items before volume v (written by the reduction)
+    BatchCtrl* ctrl;
+    unsigned long long capacity;   // vertices the outputs can hold
+    int nvol;
+    int rounds;                    // traversal rounds of 32 vertices per work item
+};
+
 cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ctas, cudaStream_t st);
+cudaError_t launch_classify_batch(const BatchDev& B, int ftype, unsigned int bricks, cudaStream_t st);
+cudaError_t launch_reduce_batch(const BatchDev& B, unsigned int chunks, cudaStream_t st);
+cudaError_t launch_traverse_batch(const BatchDev& B, const TraverseOut& O, int ftype, int normal_mode, int grid,
+                                  cudaStream_t st);
+int traverse_batch_blocks_per_sm();
 cudaError_t launch_reduce(const Volume& V, cudaStream_t st);
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st);

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "hpmc_batch.cuh"
 #include "hpmc_device.cuh"
 #include "hpmc_fetch.cuh"
 #include "hpmc_kernels.h"
@@ -193,9 +194,11 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
 
 }  // namespace
 
+// Column CTA body: footprint (fx, fy) of the slice tiles, slices
+// zc*column_slices .. +column_slices-1, field boxes from the tensor map `tmap`.
 template <int FT>
-__global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_constant__ CUtensorMap tmap,
-                                                                const __grid_constant__ Volume V) {
+__device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, const Volume& V, int fx, int fy,
+                                                     int zc) {
     using T = typename std::conditional<FT == kFieldF32, float, uint8_t>::type;
     constexpr int BXE = (FT == kFieldF32) ? 36 : 48;  // box width (16-byte multiple)
     constexpr int LAYER = BXE * 33;                    // elements of one sample layer
@@ -212,9 +215,8 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     __shared__ uint8_t s_cnt[256];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int fx = blockIdx.x, fy = blockIdx.y;
     const int x0 = fx * 32, y0 = fy * 32;
-    const int z0 = blockIdx.z * V.column_slices;
+    const int z0 = zc * V.column_slices;
     const int z1 = min(V.cells[2], z0 + V.column_slices);
     const int nlayers = z1 - z0 + 1;
     const int nbox = (nlayers + kLayersPerBox - 1) / kLayersPerBox;
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
     if (tid == 0) {
         for (int k = 0; k < kRingStages && k < nbox; k++) {
             mbar_arrive_expect_tx(&s_bar[k], STAGE_BYTES);
-            tma_load_3d(s_ring + k * STAGE_STRIDE, &tmap, x0, y0, z0 + k * kLayersPerBox, &s_bar[k]);
+            tma_load_3d(s_ring + k * STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &s_bar[k]);
         }
     }
     // cells of this lane's row inside the grid (masked codes are 0, shadergen.cpp:112-125)
@@ -276,7 +278,7 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
         if (__syncthreads_or(timed_out)) break;
         if (tid == 0 && k + kRingStages < nbox) {
             mbar_arrive_expect_tx(&s_bar[s], STAGE_BYTES);
-            tma_load_3d(s_ring + s * STAGE_STRIDE, &tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox, &s_bar[s]);
+            tma_load_3d(s_ring + s * STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox, &s_bar[s]);
         }
         // slices whose upper layer arrived in this box, warp (slice mod 8) each,
         // so the work rotates over the warps from box to box.  A warp may still
@@ -297,6 +299,12 @@ __global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_con
             atomicOr(&V.ctrl->status, kStatusTimeout);
         }
     }
+}
+
+template <int FT>
+__global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_constant__ CUtensorMap tmap,
+                                                                const __grid_constant__ Volume V) {
+    classify_column_body<FT>(&tmap, V, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,15 +406,15 @@ __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int
     }
 }
 
-__global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant__ Volume V, int j_in, int j_stop,
-                                                          int mask_level5) {
-    __shared__ __align__(16) uint32_t buf0[kReduceTop];
-    __shared__ uint32_t buf1[kReduceTop / 4];
-    __shared__ int s_last;
+// One chunk of kReduceChunk level-j_in entries (chunk `chunk` of `nchunks`).
+// Returns true in the CTA that wrote the vertex count (level jtop reached).
+__device__ __forceinline__ bool reduce_chunk(const Volume& V, int j_in, int j_stop, int mask_level5,
+                                             long long chunk, unsigned int nchunks, uint32_t* buf0, uint32_t* buf1,
+                                             int* s_last) {
     bool overflow = false;
     const long long n_in = level_entries(V.size_l2, j_in);
-    const long long base = (long long)blockIdx.x * kReduceChunk;
-    const long long n = min((long long)kReduceChunk, n_in - base);  // a power of 4 (>= 4)
+    const long long base = chunk * kReduceChunk;
+    const long long n = min((long long)kReduceChunk, n_in - base);  // a power of 4 (>= 4), or 1 at the top
     const int t = threadIdx.x;
     if (4 * t < n) {
         uint4 v = *reinterpret_cast<const uint4*>(V.levels + V.level_off[j_in] + base + 4 * t);
@@ -425,14 +433,14 @@ __global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant_
     if (j < j_stop) {
         // levels remain above this chunk's top: the last CTA to finish continues
         __threadfence();
-        if (threadIdx.x == 0) s_last = (atomicAdd(&V.ctrl->reduce_done, 1u) == gridDim.x - 1);
+        if (threadIdx.x == 0) *s_last = (atomicAdd(&V.ctrl->reduce_done, 1u) == nchunks - 1);
         __syncthreads();
-        if (!s_last) {
+        if (!*s_last) {
             if (overflow) atomicOr(&V.ctrl->status, kStatusOverflow);
-            return;
+            return false;
         }
         __threadfence();
-        const long long m = level_entries(V.size_l2, j);  // == gridDim.x entries, <= kReduceTop
+        const long long m = level_entries(V.size_l2, j);  // == nchunks entries, <= kReduceTop
         for (long long i = threadIdx.x; i < m; i += blockDim.x) buf0[i] = __ldcg(&V.levels[V.level_off[j] + i]);
         __syncthreads();
         reduce_tree(V, buf0, buf1, j, j_stop, m, 0, overflow);
@@ -440,11 +448,135 @@ __global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant_
     }
     if (overflow) atomicOr(&V.ctrl->status, kStatusOverflow);
     if (j == V.jtop && threadIdx.x == 0) V.ctrl->total = buf0[0];
+    return j == V.jtop;
+}
+
+__global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant__ Volume V, int j_in, int j_stop,
+                                                          int mask_level5) {
+    __shared__ __align__(16) uint32_t buf0[kReduceTop];
+    __shared__ uint32_t buf1[kReduceTop / 4];
+    __shared__ int s_last;
+    reduce_chunk(V, j_in, j_stop, mask_level5, blockIdx.x, gridDim.x, buf0, buf1, &s_last);
 }
 
 // Top entry when the whole pyramid is one block (no reduction launch needed).
 __global__ void copy_total(const __grid_constant__ Volume V) {
     if (threadIdx.x == 0) V.ctrl->total = V.levels[V.level_off[V.jtop]];
+}
+
+// ---------------------------------------------------------------------------
+// Batched build.  One classify launch covers the column bricks of every
+// volume (CTA = one brick, its volume found in the brick prefix array); one
+// reduce launch covers the reduction chunks of every volume (each volume's
+// pyramid finished by its own last CTA), and the CTA that completes the last
+// volume scans the per-volume counts into output offsets and traversal work
+// items.  Volume descriptors are copied into shared memory per CTA.
+template <int FT>
+__global__ void __launch_bounds__(kThreads) classify_batch_tma(const __grid_constant__ BatchDev B) {
+    __shared__ __align__(16) Volume sV;
+    const int v = find_segment(B.brick_start, B.nvol, blockIdx.x);
+    copy_volume(&sV, B.vols + v, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const uint32_t lb = blockIdx.x - __ldg(B.brick_start + v);
+    const uint32_t per_slab = (uint32_t)sV.nfx * (uint32_t)sV.nfy;
+    const int zc = (int)(lb / per_slab);
+    const uint32_t r = lb - (uint32_t)zc * per_slab;
+    const int fy = (int)(r / (uint32_t)sV.nfx);
+    const int fx = (int)(r - (uint32_t)fy * (uint32_t)sV.nfx);
+    classify_column_body<FT>(B.tmaps + v, sV, fx, fy, zc);
+}
+
+namespace {
+
+// Block-wide exclusive scan (kThreads threads); `total` receives the sum.
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T x, T* s_warp, T& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    T off = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) {
+        const T s = s_warp[w];
+        if (w < warp) off += s;
+        tot += s;
+    }
+    __syncthreads();
+    total = tot;
+    return off + inc - x;
+}
+
+// Output offsets (exclusive scan of the vertex counts) and traversal work
+// items (vertices that fit the output, in items of 32 * rounds).
+__device__ void batch_scan(const BatchDev& B) {
+    __shared__ unsigned long long s_w64[kWarps];
+    __shared__ uint32_t s_w32[kWarps];
+    const uint32_t VW = 32u * (uint32_t)B.rounds;
+    unsigned long long carry = 0;
+    uint32_t ccarry = 0;
+    for (int base = 0; base < B.nvol; base += kThreads) {
+        const int v = base + (int)threadIdx.x;
+        unsigned long long tot = 0;
+        if (v < B.nvol) {
+            const Ctrl* c = B.vols[v].ctrl;
+            tot = __ldcg(&c->total);
+        }
+        unsigned long long sum64;
+        const unsigned long long vb = carry + block_exclusive_scan<unsigned long long>(tot, s_w64, sum64);
+        const unsigned long long room = B.capacity > vb ? B.capacity - vb : 0ull;
+        const unsigned long long nw = tot < room ? tot : room;
+        const uint32_t items = (uint32_t)((nw + VW - 1) / VW);
+        uint32_t sum32;
+        const uint32_t cs = ccarry + block_exclusive_scan<uint32_t>(items, s_w32, sum32);
+        if (v < B.nvol) {
+            B.vbase[v] = vb;
+            B.chunk_start[v] = cs;
+        }
+        carry += sum64;
+        ccarry += sum32;
+    }
+    if (threadIdx.x == 0) {
+        B.vbase[B.nvol] = carry;
+        B.chunk_start[B.nvol] = ccarry;
+        B.ctrl->total = carry;
+        if (carry > B.capacity) atomicOr(&B.ctrl->status, kStatusCapacity);
+        B.ctrl->reduce_done = 0;
+        __threadfence();
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads) reduce_batch(const __grid_constant__ BatchDev B) {
+    __shared__ __align__(16) uint32_t buf0[kReduceTop];
+    __shared__ uint32_t buf1[kReduceTop / 4];
+    __shared__ __align__(16) Volume sV;
+    __shared__ int s_last, s_all;
+    const int v = find_segment(B.reduce_start, B.nvol, blockIdx.x);
+    copy_volume(&sV, B.vols + v, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const uint32_t c0 = __ldg(B.reduce_start + v);
+    const uint32_t nchunks = __ldg(B.reduce_start + v + 1) - c0;
+    // every batch volume reaches its top in this launch (jtop - 5 <= 11)
+    const bool finished = reduce_chunk(sV, kBlockLevel, sV.jtop, sV.column_layout, (long long)(blockIdx.x - c0),
+                                       nchunks, buf0, buf1, &s_last);
+    if (!finished) return;  // uniform across the CTA
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();  // this volume's total before the batch counter
+        s_all = (atomicAdd(&B.ctrl->reduce_done, 1u) == (unsigned)B.nvol - 1u);
+    }
+    __syncthreads();
+    if (s_all) {
+        __threadfence();
+        batch_scan(B);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -495,12 +627,34 @@ cudaError_t launch_reduce(const Volume& V, cudaStream_t st) {
     return cudaSuccess;
 }
 
+cudaError_t launch_classify_batch(const BatchDev& B, int ftype, unsigned int bricks, cudaStream_t st) {
+    if (!bricks) return cudaSuccess;
+    if (ftype == kFieldF32)
+        classify_batch_tma<kFieldF32><<<bricks, kThreads, kRingBytesF32, st>>>(B);
+    else if (ftype == kFieldU8)
+        classify_batch_tma<kFieldU8><<<bricks, kThreads, kRingBytesU8, st>>>(B);
+    else if (ftype == kFieldUNorm8)
+        classify_batch_tma<kFieldUNorm8><<<bricks, kThreads, kRingBytesU8, st>>>(B);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_batch(const BatchDev& B, unsigned int chunks, cudaStream_t st) {
+    reduce_batch<<<chunks, kThreads, 0, st>>>(B);
+    return cudaGetLastError();
+}
+
 bool column_smem_ok() {
     static int configured = 0;
     if (!configured) {
         cudaFuncSetAttribute(classify_column_tma<kFieldF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesF32);
         cudaFuncSetAttribute(classify_column_tma<kFieldU8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesU8);
         cudaFuncSetAttribute(classify_column_tma<kFieldUNorm8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kRingBytesU8);
+        cudaFuncSetAttribute(classify_batch_tma<kFieldF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesF32);
+        cudaFuncSetAttribute(classify_batch_tma<kFieldU8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesU8);
+        cudaFuncSetAttribute(classify_batch_tma<kFieldUNorm8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kRingBytesU8);
         configured = 1;
     }

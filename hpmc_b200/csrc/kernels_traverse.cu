@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "hpmc_batch.cuh"
 #include "hpmc_device.cuh"
 #include "hpmc_fetch.cuh"
 #include "hpmc_geometry.cuh"
@@ -68,7 +69,8 @@ __device__ __forceinline__ uint32_t compact32(uint32_t v) {
     return v;
 }
 
-__device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
+// Case tables and the block Morton table (no barrier).
+__device__ __forceinline__ void load_base_tables(TraverseSmem& S) {
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         S.cnt[i] = c_vertex_count_t[i];
         S.edge[i] = c_edge_nibbles[i];
@@ -78,6 +80,10 @@ __device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
         morton10((uint32_t)i, cx, cy);
         S.morton[i] = (uint16_t)(cx | (cy << 8));
     }
+}
+
+__device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
+    load_base_tables(S);
     for (int i = threadIdx.x; i < V.top_cached; i += blockDim.x) S.top[i] = V.levels[i];
     __syncthreads();
 }
@@ -221,6 +227,24 @@ __device__ __forceinline__ void finish_queue(const Volume& V) {
         if (atomicAdd(&V.ctrl->work_done, 1u) == gridDim.x - 1) {
             V.ctrl->work_next = 0;
             V.ctrl->work_done = 0;
+            __threadfence();
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t next_chunk_batch(const BatchDev& Bt, int lane) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&Bt.ctrl->work_next, 1u);
+    return __shfl_sync(0xffffffffu, c, 0);
+}
+
+__device__ __forceinline__ void finish_queue_batch(const BatchDev& Bt) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&Bt.ctrl->work_done, 1u) == gridDim.x - 1) {
+            Bt.ctrl->work_next = 0;
+            Bt.ctrl->work_done = 0;
             __threadfence();
         }
     }
@@ -373,6 +397,63 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
 }
 
 // ---------------------------------------------------------------------------
+// Batched traversal: one persistent grid over the work items of every volume
+// (chunk_start, written by the batched reduction).  A warp that takes an item
+// of another volume copies that volume's descriptor into its own shared slot;
+// the descriptors have top_cached = 0, so the descent reads the dense levels
+// through L1 instead of a per-CTA cache.
+template <int FT, int MODE>
+__global__ void __launch_bounds__(kThreads, 4) traverse_batch(const __grid_constant__ BatchDev Bt,
+                                                              const __grid_constant__ TraverseOut O) {
+    __shared__ __align__(16) TraverseSmem S;
+    __shared__ __align__(16) Volume s_vol[kWarps];
+    load_base_tables(S);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t VW = 32u * (uint32_t)Bt.rounds;
+    const uint32_t nitems = __ldcg(Bt.chunk_start + Bt.nvol);
+    const Volume& V = s_vol[warp];
+    int cur = -1;
+    uint32_t c0 = 0, c1 = 0, N = 0;
+    unsigned long long vb = 0;
+    WarpBlock B;
+    B.have = false;
+    for (uint32_t item = next_chunk_batch(Bt, lane); item < nitems; item = next_chunk_batch(Bt, lane)) {
+        if (cur < 0 || item < c0 || item >= c1) {
+            const int v = find_segment(Bt.chunk_start, Bt.nvol, item);
+            __syncwarp();
+            copy_volume(&s_vol[warp], Bt.vols + v, lane, 32);
+            __syncwarp();
+            cur = v;
+            c0 = __ldcg(Bt.chunk_start + v);
+            c1 = __ldcg(Bt.chunk_start + v + 1);
+            vb = __ldcg(Bt.vbase + v);
+            const unsigned long long total = __ldcg(&V.ctrl->total);
+            const unsigned long long room = Bt.capacity > vb ? Bt.capacity - vb : 0ull;
+            N = (uint32_t)(total < room ? total : room);
+            B.have = false;
+        }
+        const uint32_t first = (item - c0) * VW;
+#pragma unroll 1
+        for (int r = 0; r < Bt.rounds; r++) {
+            const uint32_t v = first + 32u * r + lane;
+            const bool act = v < N;
+            if (!__any_sync(0xffffffffu, act)) break;
+            VertexCell c;
+            if (!resolve_vertex(V, S, warp, lane, v, act, B, c)) continue;
+            const EdgeGeom g = edge_of(S, c);
+            float p[3], n[3], t;
+            edge_vertex<FT, MODE>(V, g.a, g.axis, c.x, c.y, c.z, g_binary_normals + 3 * (16 * c.code + c.k), p, n,
+                                  t);
+            const unsigned long long o = vb + v;
+            if (O.pos) __stcs(O.pos + o, make_float4(p[0], p[1], p[2], 1.0f));
+            if (O.nrm) __stcs(O.nrm + o, make_float4(n[0], n[1], n[2], 0.0f));
+        }
+    }
+    finish_queue_batch(Bt);
+}
+
+// ---------------------------------------------------------------------------
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st) {
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
@@ -414,6 +495,37 @@ cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode,
     return cudaGetLastError();
 }
 
+cudaError_t launch_traverse_batch(const BatchDev& B, const TraverseOut& O, int ftype, int normal_mode, int grid,
+                                  cudaStream_t st) {
+    const bool central = normal_mode == kNormalsCentral;
+    switch (ftype) {
+        case kFieldF32:
+            if (central) traverse_batch<kFieldF32, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
+            else traverse_batch<kFieldF32, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            break;
+        case kFieldU8:
+            if (central) traverse_batch<kFieldU8, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
+            else traverse_batch<kFieldU8, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            break;
+        case kFieldUNorm8:
+            if (central) traverse_batch<kFieldUNorm8, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
+            else traverse_batch<kFieldUNorm8, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+int traverse_batch_blocks_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_batch<kFieldF32, kModeCentral>, kThreads, 0) !=
+            cudaSuccess ||
+        n < 1)
+        n = 1;
+    return n;
+}
+
 int traverse_blocks_per_sm() {
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<kFieldF32, kModeCentral>, kThreads, 0) !=
@@ -424,3 +536,4 @@ int traverse_blocks_per_sm() {
 }
 
 }  // namespace hpmc
+

@@ -50,7 +50,7 @@ typedef enum HPMCStatus {
     HPMC_ERR_NO_FIELD = 10,       /* no field source set */
     HPMC_ERR_OVERFLOW = 11,       /* vertex count does not fit 32 bits */
     HPMC_ERR_TIMEOUT = 12,        /* a bounded device wait gave up */
-    HPMC_ERR_TOO_LARGE = 13       /* lattice needs more than the fixed scratch of HPMCextractStatic */
+    HPMC_ERR_TOO_LARGE = 13       /* lattice too large for HPMCextractStatic's fixed scratch or for a batch */
 } HPMCStatus;
 
 /* ---- field element types of device arrays ---- */
@@ -242,6 +242,61 @@ int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
  * cell block inside one slice tile, 16-byte aligned array field), 0 = generic
  * per-block kernel (narrow tiles, unaligned pitches, functor fields). */
 int HPMCgetClassifyPath(struct HPMCHistoPyramid* h, int* path);
+
+/* ---- batched extraction ----
+ *
+ * No counterpart in the reference, which builds one volume per HistoPyramid
+ * handle.  A batch holds many volumes of uneven lattices and iso-values (one
+ * scalar type per batch) and extracts all of them with three launches --
+ * classify over every volume's bricks, reduce over every volume's pyramid,
+ * one persistent traversal -- captured once in a CUDA graph and replayed.
+ * Per volume the vertices, their order and their values equal those of
+ * HPMCbuildHistopyramid + HPMCextractVerticesToBuffers on that volume.
+ * Vertices of volume v are written at [offsets[v], offsets[v+1]) of the
+ * float4 position/normal outputs (either may be NULL).  Batches are not
+ * thread-safe; calls on different streams must be ordered by the caller. */
+typedef struct HPMCBatchVolume {
+    const void* field;        /* device array, x fastest */
+    int scalar_type;          /* HPMCScalarType, the same for every volume */
+    GLsizei size[3];          /* lattice size (HPMCsetLatticeSize); grid = size - 1 */
+    size_t row_pitch_bytes;   /* 0 = dense */
+    size_t slice_pitch_bytes; /* 0 = dense */
+    GLfloat iso;              /* threshold of this volume */
+    GLfloat extent[3];        /* HPMCsetGridExtent; all zero means (1,1,1) */
+} HPMCBatchVolume;
+
+struct HPMCBatch;
+
+/* Lays out every volume (reference layout per volume) and allocates the
+ * batch.  HPMC_ERR_LAYOUT for a lattice the reference rejects,
+ * HPMC_ERR_TOO_LARGE for a volume whose base level exceeds 2^15 x 2^15
+ * texels, HPMC_ERR_INVALID_VALUE for mixed scalar types or bad pitches. */
+int HPMCcreateBatch(struct HPMCConstants* c, const HPMCBatchVolume* volumes, int count, struct HPMCBatch** out);
+void HPMCdestroyBatch(struct HPMCBatch* b);
+/* New iso-values (count entries); the fields themselves may change in place. */
+int HPMCbatchSetIsoValues(struct HPMCBatch* b, const GLfloat* iso);
+int HPMCbatchSetNormalMode(struct HPMCBatch* b, int mode);
+/* Asynchronous build + count + extraction of every volume on `cuda_stream`
+ * (a graph replay; the graph is captured again only when the outputs,
+ * capacity, normal mode or tuning change). */
+int HPMCbatchExtract(struct HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices,
+                     void* cuda_stream);
+/* count + 1 output offsets of the last extraction (the last entry is the
+ * total, which may exceed the capacity); waits for it.  Returns
+ * HPMC_ERR_CAPACITY if the outputs were too small (the vertices that fit
+ * are written). */
+int HPMCbatchGetOffsets(struct HPMCBatch* b, unsigned long long* host_offsets);
+/* Device array of the count + 1 offsets, for stream-ordered consumers. */
+int HPMCbatchGetDeviceOffsets(struct HPMCBatch* b, const unsigned long long** device_offsets);
+/* Brick depth (slices per column CTA: 7, 15, 31, 63; 0 = automatic),
+ * traversal CTAs per SM (0 = maximum) and rounds of 32 vertices per
+ * traversal work item (0 = default). */
+int HPMCbatchSetTuning(struct HPMCBatch* b, int column_slices, int traverse_ctas_per_sm, int rounds);
+int HPMCbatchGetTuning(struct HPMCBatch* b, int out[3]);
+/* Times every tuning choice on these outputs (graph replays, CUDA events)
+ * and keeps the fastest; `chosen` (may be NULL) receives it. */
+int HPMCbatchAutotune(struct HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices,
+                      void* cuda_stream, int chosen[3]);
 
 /* ---- extraction without device allocation ----
  *
