@@ -11,6 +11,9 @@ position/normal streams (HPMCextractVertices, vertex count read on the device).
   roofline the build kernels (classify + reduce) against measured HBM copy
            bandwidth; algorithmic bytes = field bytes read once
   cpu_baseline  the oracle (CPU restatement of the reference) on a z-slab sample
+  batched  64 uneven FP32 volumes: batched extractor (CUDA-graph replay) vs
+           the plain per-volume loop through the handle API, volumes/s
+  adjoint  128^3 sphere SDF: adjoint (backward) time over forward time
 
 --impl reference times the reference's path on the host cores instead: the
 reference is GLSL for a GL driver (no GL stack on this box), so its CPU
@@ -252,6 +255,64 @@ def run_batched(args, dev, stream):
             "graph": True, "steps": steps}
 
 
+def run_adjoint(args, dev, stream):
+    """Differentiable extraction on the 128^3 SDF of 16 spheres (iso 0, central
+    normals): forward = build + extraction, backward = zeroing dL/df + the
+    adjoint kernel for L = sum w.p + u.n (w, u ~ N(0,1)); CUDA events.  The
+    8 MB field stays in L2 for both passes."""
+    import torch
+
+    import hpmc_b200 as H
+    from hpmc_b200 import datasets
+
+    field_np, iso = datasets.spheres_sdf(128)
+    f = torch.from_numpy(field_np).to(dev)
+    hp = H.HistoPyramid(H.default_constants())
+    hp.set_stream(stream)
+    hp.set_field_device(f)
+    hp.set_normal_mode(H.NORMALS_CENTRAL)
+    hp.build(iso)
+    n = hp.acquire_number_of_vertices()
+    th = H.TraversalHandle(hp)
+    pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty_like(pos)
+    th.set_buffers(pos, nrm, n)
+    g = torch.Generator(device="cpu").manual_seed(4)
+    w = torch.randn((n, 4), generator=g).to(dev)
+    u = torch.randn((n, 4), generator=g).to(dev)
+    dfield = torch.zeros_like(f)
+    steps = max(5, min(args.steps, 50))
+
+    def fwd():
+        hp.build(iso)
+        th.extract()
+
+    def bwd():
+        dfield.zero_()
+        th.adjoint(w, u, n, dfield)
+
+    res = {}
+    with torch.cuda.stream(stream):
+        for name, fn in (("forward", fwd), ("backward", bwd)):
+            for _ in range(3):
+                fn()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+            res[name] = e0.elapsed_time(e1) / steps
+    th.close()
+    hp.close()
+    return {"workload": "spheres_128: FP32 128^3 SDF of 16 spheres, iso 0, central normals, "
+                        "L = sum w.p + u.n, w,u ~ N(0,1)",
+            "vertices": n, "forward_ms": res["forward"], "backward_ms": res["backward"],
+            "backward_over_forward": res["backward"] / res["forward"], "steps": steps,
+            "l2": "8 MB field resident in L2 for both passes"}
+
+
 def run_hpmc(args, rank, world, local_rank):
     import torch
 
@@ -372,6 +433,9 @@ def run_hpmc(args, rank, world, local_rank):
     batched = None
     if not args.no_batch:
         batched = run_batched(args, dev, stream)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(args, dev, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -394,6 +458,7 @@ def run_hpmc(args, rank, world, local_rank):
                 "build_ms": build_avg, "traverse_ms": trav_avg,
                 "cpu_baseline": cpu, "e2e": e2e,
                 "batched": batched,
+                "adjoint": adjoint,
                 "gpu_launches": 3 * args.steps,
                 "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
@@ -411,6 +476,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--lattice", type=int, default=512, help="lattice edge (profiling runs use smaller ones)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-extraction leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-extraction leg")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))

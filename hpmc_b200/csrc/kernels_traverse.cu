@@ -331,6 +331,7 @@ template <int FT, int MODE>
 __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_constant__ Volume V,
                                                               const __grid_constant__ AdjointIO A) {
     __shared__ __align__(16) TraverseSmem S;
+    __shared__ float S_agg[kWarps][32][6];  // cotangents of lanes sharing an edge
     load_tables(V, S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long total = V.ctrl->total;
@@ -347,15 +348,45 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
             VertexCell c;
-            if (!resolve_vertex(V, S, warp, lane, v, act, B, c)) continue;
-            const EdgeGeom g = edge_of(S, c);
+            const bool have = resolve_vertex(V, S, warp, lane, v, act, B, c);
+            // Warp aggregation: vertices on the same edge (a, axis) -- the same
+            // crossing emitted by neighbouring triangles -- have the same
+            // Jacobian, so their cotangents are summed first and one lane (the
+            // lowest of the group) scatters once for all of them.
+            EdgeGeom g{};
+            float4 dp = make_float4(0.f, 0.f, 0.f, 0.f), dn = dp;
+            unsigned long long key = ~0ull - (unsigned long long)lane;  // unique for lanes without a vertex
+            if (have) {
+                g = edge_of(S, c);
+                const unsigned long long o = V.vertex_base + v;
+                if (A.dpos) dp = __ldg(A.dpos + o);
+                if (A.dnrm) dn = __ldg(A.dnrm + o);
+                key = ((((unsigned long long)g.a[2] * (unsigned long long)V.lattice[1] + (unsigned long long)g.a[1]) *
+                            (unsigned long long)V.lattice[0] + (unsigned long long)g.a[0]) << 2) | (unsigned)g.axis;
+            }
+            const unsigned int peers = __match_any_sync(0xffffffffu, key);
+            const bool leader = have && (__ffs(peers) - 1 == lane);
+            if (__popc(peers) > 1) {
+                float* slot = S_agg[warp][lane];
+                slot[0] = dp.x; slot[1] = dp.y; slot[2] = dp.z;
+                slot[3] = dn.x; slot[4] = dn.y; slot[5] = dn.z;
+            }
+            __syncwarp();
+            if (leader && __popc(peers) > 1) {
+                unsigned int rest = peers & (peers - 1u);  // the other lanes of the group
+                while (rest) {
+                    const float* q = S_agg[warp][__ffs(rest) - 1];
+                    dp.x += q[0]; dp.y += q[1]; dp.z += q[2];
+                    dn.x += q[3]; dn.y += q[4]; dn.z += q[5];
+                    rest &= rest - 1u;
+                }
+            }
+            __syncwarp();
+            if (!leader) continue;
             const int ax = g.axis;
             const int ex = ax == 0, ey = ax == 1, ez = ax == 2;
             EdgeField F;
             gather_edge<FT, MODE == kModeCentral>(V, g.a, ax, c.x, c.y, c.z, F);
-            const unsigned long long o = V.vertex_base + v;
-            const float4 dp = A.dpos ? __ldg(A.dpos + o) : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4 dn = A.dnrm ? __ldg(A.dnrm + o) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float dpv[3] = {dp.x, dp.y, dp.z};
             const float dnv[3] = {dn.x * V.scale[0], dn.y * V.scale[1], dn.z * V.scale[2]};
             const float va = F.va, vb = F.vb;

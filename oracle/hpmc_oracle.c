@@ -22,6 +22,13 @@ extern int HPMC_triangle_table[256][16];  /* tables.cpp:38-296, Bourke case orde
 extern float HPMC_edge_table[12][4];      /* tables.cpp:299-307, shift xyz + axis  */
 extern float HPMC_midpoint_table[12][3];  /* tables.cpp:314-323                    */
 
+/* The reference's edge table (tables.cpp:299-307): per edge the shift of its
+ * first corner and its axis. */
+void oracle_edge_table(float out[48])
+{
+    memcpy(out, HPMC_edge_table, sizeof(float) * 48);
+}
+
 int oracle_max_threads(void)
 {
 #ifdef _OPENMP
@@ -171,6 +178,12 @@ static inline float sample_f(const void* field, int type, const oracle_layout_t*
 double oracle_sample(const void* field, int type, const oracle_layout_t* L, size_t rp,
                      size_t sp, long x, long y, long z)
 {
+    if (type == ORACLE_F64) {
+        x = clampl(x, 0, L->lattice[0] - 1);
+        y = clampl(y, 0, L->lattice[1] - 1);
+        z = clampl(z, 0, L->lattice[2] - 1);
+        return ((const double*)field)[(size_t)z * sp + (size_t)y * rp + (size_t)x];
+    }
     return (double)sample_f(field, type, L, rp, sp, x, y, z);
 }
 
@@ -411,6 +424,72 @@ void oracle_geometry(const void* field, int type, const oracle_layout_t* L, size
             nrm[3 * v + i] = nn[i] * scale[i];
         }
     }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Adjoint of the geometry above (no reference counterpart: the reference has
+ * no gradients).  With c = iso, t = (f_a - c)/(f_a - f_b):
+ *   dt/df_a = (c - f_b)/(f_a - f_b)^2,  dt/df_b = (f_a - c)/(f_a - f_b)^2,
+ *   p_axis = (a_axis + t) s_axis,
+ *   forward: n_i = s_i((1-t)(c - f(a+e_i)) + t(c - f(b+e_i))),
+ *   central: n_i = -s_i((1-t) g_i(a) + t g_i(b)), g_i(q) = (f(q+e_i) - f(q-e_i))/2. */
+static double* g_adj_abs; /* optional sum of |terms| per sample (error scale for FP32 checks) */
+
+static inline void scatter_add(double* g, const oracle_layout_t* L, long x, long y, long z, double v)
+{
+    x = clampl(x, 0, L->lattice[0] - 1);
+    y = clampl(y, 0, L->lattice[1] - 1);
+    z = clampl(z, 0, L->lattice[2] - 1);
+    const size_t o = ((size_t)z * (size_t)L->lattice[1] + (size_t)y) * (size_t)L->lattice[0] + (size_t)x;
+    g[o] += v;
+    if (g_adj_abs) g_adj_abs[o] += fabs(v);
+}
+
+void oracle_adjoint(const void* field, int type, const oracle_layout_t* L, size_t rp, size_t sp,
+                    float iso, int normal_mode, const float extent[3], uint64_t n,
+                    const int32_t* cell_xyz, const uint8_t* edge, const double* dpos,
+                    const double* dnrm, double* dfield, double* dfield_abs)
+{
+    g_adj_abs = dfield_abs;
+    const double c = (double)iso;
+    double scale[3];
+    for (int i = 0; i < 3; i++) scale[i] = (double)extent[i] / (double)L->cells[i];
+    for (uint64_t v = 0; v < n; v++) {
+        const float* et = HPMC_edge_table[edge[v]];
+        long a[3], b[3];
+        const int axis = (int)et[3];
+        for (int i = 0; i < 3; i++) {
+            a[i] = cell_xyz[3 * v + i] + (long)et[i];
+            b[i] = a[i] + (i == axis ? 1 : 0);
+        }
+        const double va = oracle_sample(field, type, L, rp, sp, a[0], a[1], a[2]);
+        const double vb = oracle_sample(field, type, L, rp, sp, b[0], b[1], b[2]);
+        const double den = va - vb;
+        const double t = (va - c) / den;
+        double dLdt = dpos[3 * v + axis] * scale[axis];
+        for (int i = 0; i < 3; i++) {
+            const double dn = dnrm[3 * v + i] * scale[i];
+            const long e[3] = {i == 0, i == 1, i == 2};
+            const double fa = oracle_sample(field, type, L, rp, sp, a[0] + e[0], a[1] + e[1], a[2] + e[2]);
+            const double fb = oracle_sample(field, type, L, rp, sp, b[0] + e[0], b[1] + e[1], b[2] + e[2]);
+            if (normal_mode == ORACLE_NORMALS_FORWARD) {
+                dLdt += dn * (fa - fb);
+                scatter_add(dfield, L, a[0] + e[0], a[1] + e[1], a[2] + e[2], -(1.0 - t) * dn);
+                scatter_add(dfield, L, b[0] + e[0], b[1] + e[1], b[2] + e[2], -t * dn);
+            } else {
+                const double fam = oracle_sample(field, type, L, rp, sp, a[0] - e[0], a[1] - e[1], a[2] - e[2]);
+                const double fbm = oracle_sample(field, type, L, rp, sp, b[0] - e[0], b[1] - e[1], b[2] - e[2]);
+                dLdt += dn * (0.5 * (fa - fam) - 0.5 * (fb - fbm));
+                scatter_add(dfield, L, a[0] + e[0], a[1] + e[1], a[2] + e[2], -0.5 * (1.0 - t) * dn);
+                scatter_add(dfield, L, a[0] - e[0], a[1] - e[1], a[2] - e[2], 0.5 * (1.0 - t) * dn);
+                scatter_add(dfield, L, b[0] + e[0], b[1] + e[1], b[2] + e[2], -0.5 * t * dn);
+                scatter_add(dfield, L, b[0] - e[0], b[1] - e[1], b[2] - e[2], 0.5 * t * dn);
+            }
+        }
+        scatter_add(dfield, L, a[0], a[1], a[2], dLdt * (c - vb) / (den * den));
+        scatter_add(dfield, L, b[0], b[1], b[2], dLdt * (va - c) / (den * den));
+    }
+    g_adj_abs = NULL;
 }
 
 /* ------------------------------------------------------------------------- */

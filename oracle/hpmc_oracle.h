@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-enum { ORACLE_F32 = 0, ORACLE_U8 = 1, ORACLE_UNORM8 = 2 };
+enum { ORACLE_F32 = 0, ORACLE_U8 = 1, ORACLE_UNORM8 = 2, ORACLE_F64 = 3 /* geometry and adjoint only */ };
 enum { ORACLE_NORMALS_FORWARD = 0, ORACLE_NORMALS_CENTRAL = 1 };
 
 typedef struct {
@@ -113,10 +113,21 @@ void oracle_geometry(const void* field, int type, const oracle_layout_t* L,
  * CPU baseline.  Allocates internally; returns the vertex count and, if
  * pos/nrm are non-NULL and capacity suffices, FP32 positions/normals (xyz,
  * 3 floats per vertex).  threads <= 0 uses all OpenMP threads. */
+/* Adjoint of oracle_geometry for continuous fields, in FP64: accumulates
+ * dL/df = sum_v dL/dp_v . dp_v/df + dL/dn_v . dn_v/df into dfield (dense,
+ * lattice shape, x fastest).  dpos/dnrm: 3 doubles per vertex.  A clamped
+ * fetch passes its gradient to the sample it read.  dfield_abs (may be NULL)
+ * accumulates the absolute values of the same terms. */
+void oracle_adjoint(const void* field, int type, const oracle_layout_t* L, size_t rp, size_t sp,
+                    float iso, int normal_mode, const float extent[3], uint64_t n,
+                    const int32_t* cell_xyz, const uint8_t* edge, const double* dpos,
+                    const double* dnrm, double* dfield, double* dfield_abs);
+
 uint64_t oracle_extract(const void* field, int type, const int lattice[3], const int cells[3],
                         float iso, int binary, int normal_mode, const float extent[3],
                         float* pos, float* nrm, uint64_t capacity, int threads);
 
+void oracle_edge_table(float out[48]);
 int oracle_max_threads(void);
 
 #ifdef __cplusplus

@@ -18,7 +18,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REF_DIR = os.path.join(_HERE, "_ref")
 
-F32, U8, UNORM8 = 0, 1, 2
+F32, U8, UNORM8, F64 = 0, 1, 2, 3  # F64: geometry and adjoint only
 NORMALS_FORWARD, NORMALS_CENTRAL = 0, 1
 
 
@@ -92,6 +92,9 @@ def lib():
                                      vp, C.c_uint64, C.c_int]
         L.oracle_extract.restype = C.c_uint64
         L.oracle_max_threads.restype = C.c_int
+        L.oracle_edge_table.argtypes = [vp]
+        L.oracle_adjoint.argtypes = [vp, C.c_int, C.POINTER(_Layout), C.c_size_t, C.c_size_t, C.c_float, C.c_int,
+                                     fp, C.c_uint64, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -188,6 +191,8 @@ def tables():
 def _field_type(field: np.ndarray, unorm: bool) -> int:
     if field.dtype == np.float32:
         return F32
+    if field.dtype == np.float64:
+        return F64
     if field.dtype == np.uint8:
         return UNORM8 if unorm else U8
     raise TypeError(f"unsupported field dtype {field.dtype}")
@@ -258,6 +263,26 @@ def geometry(field, L: Layout, iso, cell, code, k, edge, *, binary=False,
     return t, pos, nrm
 
 
+def adjoint(field, L: Layout, iso, cell, edge, dpos, dnrm, *, normal_mode=NORMALS_FORWARD,
+            extent=(1.0, 1.0, 1.0), unorm=False, with_abs=False):
+    """FP64 dL/df of L = sum dpos.p + dnrm.n over the vertices (cell, edge);
+    dpos, dnrm are (n, 3).  Returns an array of the field's shape (float64),
+    and with_abs also the per-sample sum of |terms|."""
+    field = np.ascontiguousarray(field)
+    n = len(edge)
+    fx, fy, _ = L.lattice
+    s = _struct(L)
+    out = np.zeros(field.shape, np.float64)
+    absum = np.zeros(field.shape, np.float64) if with_abs else None
+    lib().oracle_adjoint(_ptr(field), _field_type(field, unorm), C.byref(s), fx, fx * fy, float(iso),
+                         int(normal_mode), (C.c_float * 3)(*extent), n, _ptr(np.ascontiguousarray(cell)),
+                         _ptr(np.ascontiguousarray(edge)),
+                         _ptr(np.ascontiguousarray(dpos, dtype=np.float64)),
+                         _ptr(np.ascontiguousarray(dnrm, dtype=np.float64)), _ptr(out),
+                         _ptr(absum) if with_abs else None)
+    return (out, absum) if with_abs else out
+
+
 def cell_key(L: Layout, x: int, y: int, z: int) -> int:
     s = _struct(L)
     return int(lib().oracle_cell_key(C.byref(s), x, y, z))
@@ -284,6 +309,13 @@ def extract_count(field, iso, cells=None, *, binary=False, normal_mode=NORMALS_F
     if geometry:
         return int(n), pos[:n], nrm[:n]
     return int(n), None, None
+
+
+def edge_table() -> np.ndarray:
+    """The reference's edge table, (12, 4): first-corner shift x, y, z and axis."""
+    out = np.zeros(48, np.float32)
+    lib().oracle_edge_table(_ptr(out))
+    return out.reshape(12, 4)
 
 
 def max_threads() -> int:
