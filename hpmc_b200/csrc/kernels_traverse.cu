@@ -13,13 +13,16 @@
 //      running sum exceeds the key exactly as shadergen.cpp:448-467 does.  All
 //      lanes walk the same path, so every load is one broadcast transaction;
 //      consecutive vertices reuse the block and skip the descent.
-//   2. in-block lookup (warp-cooperative): the warp loads the block's 1024
-//      codes from the arena, each lane turns 32 of them into vertex counts, a
-//      warp scan gives the block's per-cell prefix sums in shared memory, and
-//      each lane binary-searches its key (shadergen.cpp:469-495).
+//   2. in-block lookup (warp-cooperative; replaces the base-level steps of
+//      shadergen.cpp:469-495): on entering a block the warp turns its 1024
+//      codes into the list of active cells (count > 0) with their first
+//      vertex, in vertex order; per round a lane's cell is found from the
+//      list with one OR-reduction of the cell starts that fall in the
+//      round's window and a popcount (no per-vertex search).
 //   3. geometry (shadergen.cpp:497-563): edge from the case table, crossing
-//      parameter t, position and normal; FP32 samples and outputs with FP64
-//      intermediates; coalesced streaming float4 stores.
+//      parameter t, position and normal; FP32 arithmetic with a float-float
+//      fallback for ill-conditioned normals; coalesced streaming float4
+//      stores.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -43,20 +46,28 @@ namespace {
 
 struct TraverseSmem {
     uint64_t edge[256];
-    uint32_t codew[kWarps][kBlockWords];
-    uint16_t pref[kWarps][kBlockKeys];
+    // active cells (vertex count > 0) of each warp's block, in vertex order:
+    // start << 18 | code << 10 | cell (start = first block-relative vertex of
+    // the cell, <= 15 * 1024; cell = Morton index of the cell in the block)
+    uint32_t act[kWarps][kBlockKeys];
     uint32_t top[kTopCacheEntries];
     uint16_t morton[kBlockKeys];  // cell Morton index in a block -> cx | cy << 8
     uint8_t cnt[256];
 };
 
+constexpr size_t kTraverseSmem = sizeof(TraverseSmem);
+constexpr size_t kBatchVolOffset = (sizeof(TraverseSmem) + 15) & ~size_t(15);
+constexpr size_t kBatchSmem = kBatchVolOffset + kWarps * sizeof(Volume);
+
 // The block a warp is working in: its key-space origin and, for the column
 // layout, the lattice cell of its first key (every cell of such a block lies
-// in the same slice tile).
+// in the same slice tile); its active-cell count and the active cell holding
+// the next block-relative vertex the warp expects (knext).
 struct WarpBlock {
     uint32_t b, base, count;
     uint32_t X0, Y0;
     int ox, oy, oz;
+    uint32_t nact, cur, knext;
     bool have;
 };
 
@@ -111,33 +122,59 @@ __device__ __forceinline__ void descend(const Volume& V, const TraverseSmem& S, 
     block = node;
 }
 
-// Warp-cooperative: per-cell inclusive prefix of vertex counts of block b.
-__device__ __forceinline__ void load_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t b) {
+// Warp-cooperative: the active-cell list of block b (S.act[warp]); returns
+// its length.  Lane l turns the block's codes 32l .. 32l+31 (Morton order)
+// into counts; one warp scan gives every lane its first vertex and first
+// list slot.
+__device__ __forceinline__ uint32_t load_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t b) {
     const long long slot = block_slot(V, b);
     const uint4* src = reinterpret_cast<const uint4*>(V.arena + slot * kBlockWords) + 2 * lane;
     const uint4 w0 = __ldg(src), w1 = __ldg(src + 1);
     const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-    uint32_t run = 0;
+    uint32_t vsum = 0, amask = 0;
 #pragma unroll
-    for (int i = 0; i < 32; i++) run += S.cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
-    uint32_t scan = run;  // inclusive scan of the lane sums
+    for (int i = 0; i < 32; i++) {
+        const uint32_t c = S.cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        vsum += c;
+        if (c) amask |= 1u << i;
+    }
+    // one scan of (active cells << 16 | vertices); block totals < 2^16 each
+    const uint32_t mine = vsum | ((uint32_t)__popc(amask) << 16);
+    uint32_t scan = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
         if (lane >= o) scan += t;
     }
-    uint32_t acc = scan - run;
-    uint32_t* pref32 = reinterpret_cast<uint32_t*>(&S.pref[warp][32 * lane]);
+    const uint32_t excl = scan - mine;
+    uint32_t vpos = excl & 0xffffu, apos = excl >> 16;
+    uint32_t* act = S.act[warp];
+    __syncwarp();  // every lane is done with the previous list
 #pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const uint32_t a = acc + S.cnt[(w[i >> 1] >> (16 * (i & 1))) & 0xffu];
-        acc = a + S.cnt[(w[i >> 1] >> (16 * (i & 1) + 8)) & 0xffu];
-        pref32[i] = a | (acc << 16);
+    for (int k = 0; k < 8; k++) {
+        uint32_t am = (amask >> (4 * k)) & 0xfu;
+        while (am) {
+            const int j = __ffs(am) - 1;
+            am &= am - 1u;
+            const uint32_t code = (w[k] >> (8 * j)) & 0xffu;
+            act[apos++] = (vpos << 18) | (code << 10) | (uint32_t)(32 * lane + 4 * k + j);
+            vpos += S.cnt[code];
+        }
     }
-    uint4* cw = reinterpret_cast<uint4*>(&S.codew[warp][8 * lane]);
-    cw[0] = w0;
-    cw[1] = w1;
     __syncwarp();
+    return __shfl_sync(0xffffffffu, scan, 31) >> 16;
+}
+
+// Warp-uniform: index of the active cell holding block-relative vertex k
+// (the last entry whose start is <= k), 32 entries per vote.
+__device__ __forceinline__ uint32_t find_active(const uint32_t* act, uint32_t nact, uint32_t k, int lane) {
+    for (uint32_t q = 0; q <= nact; q += 32) {
+        const uint32_t j = q + (uint32_t)lane;
+        const bool le = j < nact && (act[j] >> 18) <= k;
+        const uint32_t bal = __ballot_sync(0xffffffffu, le);
+        if (bal != 0xffffffffu) return q + (uint32_t)__popc(bal) - 1u;
+    }
+    return nact - 1u;
 }
 
 // Resolved vertex: cell, code, vertex index inside the cell.
@@ -147,60 +184,69 @@ struct VertexCell {
     int k;
 };
 
-__device__ __forceinline__ VertexCell find_cell(const Volume& V, const TraverseSmem& S, int warp,
-                                                const WarpBlock& B, uint32_t key) {
-    const uint16_t* pref = S.pref[warp];
-    int lo = 0;
-#pragma unroll
-    for (int step = 512; step >= 1; step >>= 1)
-        if (pref[lo + step - 1] <= key) lo += step;
-    VertexCell r;
-    r.code = (S.codew[warp][lo >> 2] >> (8 * (lo & 3))) & 0xff;
-    r.k = (int)key - ((int)pref[lo] - (int)S.cnt[r.code]);
-    r.k = min(max(r.k, 0), 15);  // in range whenever key < block count (table reads stay in bounds)
-    const uint32_t m = S.morton[lo];
-    const int cx = (int)(m & 0xffu), cy = (int)(m >> 8);
-    if (V.column_layout) {
-        r.x = B.ox + cx;
-        r.y = B.oy + cy;
-        r.z = B.oz;
-    } else {
-        virtual_to_cell(V, B.X0 + (uint32_t)cx, B.Y0 + (uint32_t)cy, r.x, r.y, r.z);
-    }
-    return r;
-}
-
-// Steps 1-2 for one round of 32 vertices of a warp; returns false for lanes
-// without a vertex.  B is the warp's cached block.
 __device__ __forceinline__ void enter_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t key,
                                             WarpBlock& B) {
     descend(V, S, key, B.b, B.base, B.count);  // uniform across the warp
-    load_block(V, S, warp, lane, B.b);
+    B.nact = load_block(V, S, warp, lane, B.b);
     B.X0 = compact32(B.b) << 5;
     B.Y0 = compact32(B.b >> 1) << 5;
     virtual_to_cell(V, B.X0, B.Y0, B.ox, B.oy, B.oz);
     B.have = true;
+    const uint32_t k = key - B.base;
+    B.cur = k == 0 ? 0u : find_active(S.act[warp], B.nact, k, lane);
+    B.knext = k;
 }
 
+// Steps 1-2 for one round of consecutive vertices (lane l holds vertex v,
+// lanes with `act` form a prefix of the warp).  Per pass over the lanes that
+// lie in the current block, lane j reads list entry cur+1+j; the cells that
+// start inside the pass's window of 32 vertices set one bit each, and a
+// lane's cell is cur + (starts at or before its offset) -- one popcount
+// instead of a search.  Returns `act`.
 __device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t v,
                                                bool act, WarpBlock& B, VertexCell& out) {
-    const unsigned int actm = __ballot_sync(0xffffffffu, act);
-    // common case: the whole round lies in the cached block
-    const uint32_t vfirst = __shfl_sync(0xffffffffu, v, __ffs(actm) - 1);
-    const uint32_t vlast = __shfl_sync(0xffffffffu, v, 31 - __clz(actm));
-    if (B.have && vfirst >= B.base && vlast - B.base < B.count) {
-        if (act) out = find_cell(V, S, warp, B, v - B.base);
-        return act;
-    }
-    unsigned int pending = actm;
+    unsigned int pending = __ballot_sync(0xffffffffu, act);
+    const uint32_t* list = S.act[warp];
     while (pending) {
         const int leader = __ffs(pending) - 1;
         const uint32_t vl = __shfl_sync(0xffffffffu, v, leader);
-        if (!B.have || vl < B.base || vl - B.base >= B.count) enter_block(V, S, warp, lane, vl, B);
-        const bool mine = ((pending >> lane) & 1u) && v >= B.base && v - B.base < B.count;
-        if (mine) out = find_cell(V, S, warp, B, v - B.base);
-        pending &= ~__ballot_sync(0xffffffffu, mine);
-        __syncwarp();
+        if (!B.have || vl < B.base || vl - B.base >= B.count) {
+            enter_block(V, S, warp, lane, vl, B);
+        } else if (vl - B.base != B.knext) {
+            B.cur = find_active(list, B.nact, vl - B.base, lane);
+            B.knext = vl - B.base;
+        }
+        const uint32_t k0 = B.knext;
+        const uint32_t npend = (uint32_t)__popc(pending);
+        const uint32_t left = B.count - k0;
+        const uint32_t nm = npend < left ? npend : left;  // lanes leader .. leader+nm-1
+        const int d = lane - leader;
+        const bool mine = d >= 0 && (uint32_t)d < nm;
+        const uint32_t j = B.cur + 1u + (uint32_t)lane;
+        const uint32_t pos = (j < B.nact) ? (list[j] >> 18) - k0 : 0xffffffffu;  // >= 1
+        const uint32_t starts = __reduce_or_sync(0xffffffffu, pos < 32u ? (1u << pos) : 0u);
+        if (mine) {
+            const uint32_t idx = B.cur + (uint32_t)__popc(starts & ((2u << d) - 1u));
+            const uint32_t e = list[idx];
+            out.code = (int)((e >> 10) & 0xffu);
+            out.k = (int)(k0 + (uint32_t)d - (e >> 18));
+            out.k = min(max(out.k, 0), 15);  // in range for consistent data; keeps table reads in bounds
+            const uint32_t m = S.morton[e & 0x3ffu];
+            const int cx = (int)(m & 0xffu), cy = (int)(m >> 8);
+            if (V.column_layout) {
+                out.x = B.ox + cx;
+                out.y = B.oy + cy;
+                out.z = B.oz;
+            } else {
+                virtual_to_cell(V, B.X0 + (uint32_t)cx, B.Y0 + (uint32_t)cy, out.x, out.y, out.z);
+            }
+        }
+        // the active cell of vertex k0 + nm: the last cell of the pass, or the
+        // next one if it starts exactly there
+        const bool next_starts = __any_sync(0xffffffffu, pos == nm);
+        B.cur += (uint32_t)__popc(starts & ((2u << (nm - 1u)) - 1u)) + (next_starts ? 1u : 0u);
+        B.knext = k0 + nm;
+        pending &= ~(nm >= 32u ? 0xffffffffu : (((1u << nm) - 1u) << leader));
     }
     return act;
 }
@@ -267,7 +313,8 @@ __device__ __forceinline__ EdgeGeom edge_of(const TraverseSmem& S, const VertexC
 template <int FT, int MODE>
 __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_constant__ Volume V,
                                                                const __grid_constant__ TraverseOut O) {
-    __shared__ __align__(16) TraverseSmem S;
+    extern __shared__ __align__(16) uint8_t s_traverse[];
+    TraverseSmem& S = *reinterpret_cast<TraverseSmem*>(s_traverse);
     load_tables(V, S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long total = V.ctrl->total;
@@ -330,7 +377,8 @@ __device__ __forceinline__ void scatter(const Volume& V, float* dfield, const in
 template <int FT, int MODE>
 __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_constant__ Volume V,
                                                               const __grid_constant__ AdjointIO A) {
-    __shared__ __align__(16) TraverseSmem S;
+    extern __shared__ __align__(16) uint8_t s_traverse[];
+    TraverseSmem& S = *reinterpret_cast<TraverseSmem*>(s_traverse);
     __shared__ float S_agg[kWarps][32][6];  // cotangents of lanes sharing an edge
     load_tables(V, S);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -436,8 +484,10 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
 template <int FT, int MODE>
 __global__ void __launch_bounds__(kThreads, 4) traverse_batch(const __grid_constant__ BatchDev Bt,
                                                               const __grid_constant__ TraverseOut O) {
-    __shared__ __align__(16) TraverseSmem S;
-    __shared__ __align__(16) Volume s_vol[kWarps];
+    // dynamic: TraverseSmem, then one volume descriptor per warp
+    extern __shared__ __align__(16) uint8_t s_traverse[];
+    TraverseSmem& S = *reinterpret_cast<TraverseSmem*>(s_traverse);
+    Volume* s_vol = reinterpret_cast<Volume*>(s_traverse + kBatchVolOffset);
     load_base_tables(S);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -490,9 +540,9 @@ cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mo
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
 #define HPMC_TRAVERSE_CASE(FT_)                                                                        \
     case FT_:                                                                                          \
-        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, 0, st>>>(V, O);   \
-        else if (mode == kModeCentral) traverse_kernel<FT_, kModeCentral><<<grid, kThreads, 0, st>>>(V, O); \
-        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, 0, st>>>(V, O);                     \
+        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, kTraverseSmem, st>>>(V, O);   \
+        else if (mode == kModeCentral) traverse_kernel<FT_, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, O); \
+        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, kTraverseSmem, st>>>(V, O);                     \
         break;
     switch (V.ftype) {
         HPMC_TRAVERSE_CASE(kFieldF32)
@@ -509,16 +559,16 @@ cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode,
     const bool central = normal_mode == kNormalsCentral;
     switch (V.ftype) {
         case kFieldF32:
-            if (central) adjoint_kernel<kFieldF32, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
-            else adjoint_kernel<kFieldF32, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            if (central) adjoint_kernel<kFieldF32, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
+            else adjoint_kernel<kFieldF32, kModeForward><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
             break;
         case kFieldU8:
-            if (central) adjoint_kernel<kFieldU8, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
-            else adjoint_kernel<kFieldU8, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            if (central) adjoint_kernel<kFieldU8, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
+            else adjoint_kernel<kFieldU8, kModeForward><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
             break;
         case kFieldUNorm8:
-            if (central) adjoint_kernel<kFieldUNorm8, kModeCentral><<<grid, kThreads, 0, st>>>(V, A);
-            else adjoint_kernel<kFieldUNorm8, kModeForward><<<grid, kThreads, 0, st>>>(V, A);
+            if (central) adjoint_kernel<kFieldUNorm8, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
+            else adjoint_kernel<kFieldUNorm8, kModeForward><<<grid, kThreads, kTraverseSmem, st>>>(V, A);
             break;
         default:
             return cudaErrorInvalidValue;
@@ -526,21 +576,38 @@ cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode,
     return cudaGetLastError();
 }
 
+// The batched traversal needs more than the default 48 KB of dynamic shared memory.
+static void configure_batch_smem() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    const int bytes = (int)kBatchSmem;
+    cudaFuncSetAttribute(traverse_batch<kFieldF32, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(traverse_batch<kFieldF32, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(traverse_batch<kFieldU8, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(traverse_batch<kFieldU8, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(traverse_batch<kFieldUNorm8, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         bytes);
+    cudaFuncSetAttribute(traverse_batch<kFieldUNorm8, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         bytes);
+}
+
 cudaError_t launch_traverse_batch(const BatchDev& B, const TraverseOut& O, int ftype, int normal_mode, int grid,
                                   cudaStream_t st) {
+    configure_batch_smem();  // set before any capture: the first call comes from traverse_batch_blocks_per_sm
     const bool central = normal_mode == kNormalsCentral;
     switch (ftype) {
         case kFieldF32:
-            if (central) traverse_batch<kFieldF32, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
-            else traverse_batch<kFieldF32, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            if (central) traverse_batch<kFieldF32, kModeCentral><<<grid, kThreads, kBatchSmem, st>>>(B, O);
+            else traverse_batch<kFieldF32, kModeForward><<<grid, kThreads, kBatchSmem, st>>>(B, O);
             break;
         case kFieldU8:
-            if (central) traverse_batch<kFieldU8, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
-            else traverse_batch<kFieldU8, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            if (central) traverse_batch<kFieldU8, kModeCentral><<<grid, kThreads, kBatchSmem, st>>>(B, O);
+            else traverse_batch<kFieldU8, kModeForward><<<grid, kThreads, kBatchSmem, st>>>(B, O);
             break;
         case kFieldUNorm8:
-            if (central) traverse_batch<kFieldUNorm8, kModeCentral><<<grid, kThreads, 0, st>>>(B, O);
-            else traverse_batch<kFieldUNorm8, kModeForward><<<grid, kThreads, 0, st>>>(B, O);
+            if (central) traverse_batch<kFieldUNorm8, kModeCentral><<<grid, kThreads, kBatchSmem, st>>>(B, O);
+            else traverse_batch<kFieldUNorm8, kModeForward><<<grid, kThreads, kBatchSmem, st>>>(B, O);
             break;
         default:
             return cudaErrorInvalidValue;
@@ -549,8 +616,10 @@ cudaError_t launch_traverse_batch(const BatchDev& B, const TraverseOut& O, int f
 }
 
 int traverse_batch_blocks_per_sm() {
+    configure_batch_smem();
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_batch<kFieldF32, kModeCentral>, kThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_batch<kFieldF32, kModeCentral>, kThreads,
+                                                      kBatchSmem) !=
             cudaSuccess ||
         n < 1)
         n = 1;
@@ -559,7 +628,8 @@ int traverse_batch_blocks_per_sm() {
 
 int traverse_blocks_per_sm() {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<kFieldF32, kModeCentral>, kThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, traverse_kernel<kFieldF32, kModeCentral>, kThreads,
+                                                      kTraverseSmem) !=
             cudaSuccess ||
         n < 1)
         n = 1;
