@@ -213,9 +213,10 @@ bool setup(HPMCHistoPyramid* h) {
     V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
     V.nfx = (V.cells[0] + 31) / 32;
     V.nfy = (V.cells[1] + 31) / 32;
-    // slices per column CTA: the longest column that still gives ~12 CTAs per SM
+    // slices per column: the longest column that still gives the persistent
+    // classifier (2 CTAs per SM) ~12 columns per CTA
     {
-        const long long target = 12ll * h->constants->num_sms;
+        const long long target = 24ll * h->constants->num_sms;
         V.column_slices = hpmc::kColumnSliceChoices[3];
         for (int zc : hpmc::kColumnSliceChoices) {
             if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= target) {

@@ -2,7 +2,7 @@
 // with the first five reductions, then the upper reductions.
 //
 // Reference passes replaced (hpmc/src/buildpass.cpp:42-178):
-//   base level  (shadergen.cpp:86-171)  -> classify_column_tma / classify_blocks
+//   base level  (shadergen.cpp:86-171)  -> classify_columns / classify_blocks
 //   first reduction + 4 upper levels    -> fused into classification (a 32x32
 //                                          cell block = 4^5 keys is summed in
 //                                          registers and warp reductions)
@@ -168,16 +168,19 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
         const uint32_t qy = (uint32_t)lane >> 1;
         const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
         uint32_t* dst = V.arena + slot * kBlockWords;
+        // Morton index of quad (qx, qy), qx = (odd ? 8 : 0) + i: the bits of i
+        // (compile-time) and of the lane's part are disjoint
+        const uint32_t qys = (qy & 1u) | ((qy & 2u) << 1) | ((qy & 4u) << 2) | ((qy & 8u) << 3);
+        const uint32_t qbase = (odd ? 0x40u : 0u) | (qys << 1);
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const uint32_t qx = (odd ? 8u : 0u) + (uint32_t)i;
             const uint32_t wi = odd ? w[4 + (i >> 1)] : w[i >> 1];  // this lane's word with cells 2qx, 2qx+1
             const uint32_t pi = odd ? p[4 + (i >> 1)] : p[i >> 1];
             const uint32_t upper = odd ? wi : pi;  // row 2qy+1
             const uint32_t lower = odd ? pi : wi;  // row 2qy
             const uint32_t word = __byte_perm(lower, upper, (i & 1) ? 0x7632 : 0x5410);
-            const uint32_t q = (uint32_t)(morton_spread(qx) | (morton_spread(qy) << 1));
-            dst[q] = word;
+            const uint32_t ispread = (uint32_t)((i & 1) | ((i & 2) << 1) | ((i & 4) << 2));
+            dst[qbase | ispread] = word;
         }
     }
     if (V.codes_out) {
@@ -194,25 +197,99 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
 
 }  // namespace
 
-// Column CTA body: footprint (fx, fy) of the slice tiles, slices
-// zc*column_slices .. +column_slices-1, field boxes from the tensor map `tmap`.
-template <int FT>
-__device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, const Volume& V, int fx, int fy,
-                                                     int zc) {
-    using T = typename std::conditional<FT == kFieldF32, float, uint8_t>::type;
-    constexpr int BXE = (FT == kFieldF32) ? 36 : 48;  // box width (16-byte multiple)
-    constexpr int LAYER = BXE * 33;                    // elements of one sample layer
-    constexpr int STAGE_BYTES = LAYER * kLayersPerBox * (int)sizeof(T);
-    constexpr int STAGE_STRIDE = (STAGE_BYTES + 127) & ~127;
+// Shared memory of a column classifier CTA.  Bit rows are kept for the last
+// kRowBuffers sample layers (indexed by a running layer counter mod
+// kRowBuffers): while a slow warp still classifies the slices of box p
+// (layers 8p-1 .. 8p+7) other warps already convert box p+1 (layers 8p+8 ..
+// 8p+15), so the buffers of the two boxes must not alias.
+constexpr int kRowBuffers = 32;
 
+template <int FT>
+struct ColumnGeom {
+    using T = typename std::conditional<FT == kFieldF32, float, uint8_t>::type;
+    static constexpr int BXE = (FT == kFieldF32) ? 36 : 48;  // box width (16-byte multiple)
+    static constexpr int LAYER = BXE * 33;                    // elements of one sample layer
+    static constexpr int STAGE_BYTES = LAYER * kLayersPerBox * (int)sizeof(T);
+    static constexpr int STAGE_STRIDE = (STAGE_BYTES + 127) & ~127;
+};
+
+struct ColumnSmem {
+    uint64_t bar[kRingStages];
+    uint32_t rows[kRowBuffers][36];  // bit x = sample (x0 + x, y0 + r) below iso; [32] = row 32
+    uint64_t col[kRowBuffers];       // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
+    uint8_t cnt[256];
+};
+
+// Bit rows of the nl layers of one box (stage st), layer l stored at
+// running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
+// row 32 and column x0+32 of layer g go to warp (g + 3) mod 8.
+template <int FT>
+__device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st, int nl, uint32_t gl0, float iso,
+                                            int u8_thr, int warp, int lane, ColumnSmem& C) {
+    using G = ColumnGeom<FT>;
+#pragma unroll
+    for (int l = 0; l < kLayersPerBox; l++) {
+        if (l < nl) {
+            const typename G::T* layer = st + l * G::LAYER;
+            const uint32_t buf = (gl0 + l) & (kRowBuffers - 1);
+            const typename G::T* row = layer + 4 * warp * G::BXE + lane;
+            const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(row[0], iso, u8_thr));
+            const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(row[G::BXE], iso, u8_thr));
+            const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(row[2 * G::BXE], iso, u8_thr));
+            const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(row[3 * G::BXE], iso, u8_thr));
+            if (lane == 0) *reinterpret_cast<uint4*>(&C.rows[buf][4 * warp]) = make_uint4(b0, b1, b2, b3);
+            if (warp == (int)((gl0 + l + 3) & 7)) {
+                const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(layer[32 * G::BXE + lane], iso, u8_thr));
+                const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(layer[lane * G::BXE + 32], iso, u8_thr));
+                const bool corner = below<FT>(layer[32 * G::BXE + 32], iso, u8_thr);
+                if (lane == 0) {
+                    C.rows[buf][32] = r32;
+                    C.col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
+                }
+            }
+        }
+    }
+}
+
+// After the box barrier: the slices whose upper layer arrived in this box
+// (column-relative slices lb-1 .. lb+nl-2), warp (glu + slice) mod 8 each, so
+// the work rotates over the warps from box to box.  glu = running index of
+// the column's layer 0.
+__device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, int lb, int nl,
+                                                    uint32_t glu, int warp, int lane, uint32_t vmask,
+                                                    const ColumnSmem& C) {
+    // the slice of this warp, if any
+    const int sl = lb - 1 + (int)(((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u);
+    if (sl >= 0 && sl <= lb + nl - 2) {
+        const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
+        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt], C.cnt);
+    }
+}
+
+// Cells of row `lane` of footprint (x0, y0) inside the grid (masked codes are
+// 0, shadergen.cpp:112-125).
+__device__ __forceinline__ uint32_t row_mask(const Volume& V, int x0, int y0, int lane) {
+    const int xv = V.cells[0] - x0;
+    const uint32_t xmask = xv >= 32 ? 0xffffffffu : ((1u << xv) - 1u);
+    return (y0 + lane < V.cells[1]) ? xmask : 0u;
+}
+
+template <int FT>
+__device__ __forceinline__ uint8_t* ring_base() {
     extern __shared__ __align__(128) uint8_t s_dyn[];
     // TMA destinations must be 128-byte aligned: align the ring explicitly
     // (the launch reserves 128 spare bytes)
-    uint8_t* const s_ring = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
-    __shared__ __align__(8) uint64_t s_bar[kRingStages];
-    __shared__ __align__(16) uint32_t s_rows[16][36];  // layer % 16: bit x = sample (x0 + x, y0 + r) below iso
-    __shared__ uint64_t s_col[16];                      // layer % 16: bit r = sample (x0 + 32, y0 + r) below iso
-    __shared__ uint8_t s_cnt[256];
+    return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 127) & ~uintptr_t(127));
+}
+
+// Column CTA body (one column per CTA): footprint (fx, fy) of the slice
+// tiles, slices zc*column_slices .. +column_slices-1, field boxes from `tmap`.
+template <int FT>
+__device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, const Volume& V, int fx, int fy,
+                                                     int zc) {
+    using G = ColumnGeom<FT>;
+    uint8_t* const s_ring = ring_base<FT>();
+    __shared__ __align__(16) ColumnSmem C;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int x0 = fx * 32, y0 = fy * 32;
@@ -223,22 +300,19 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
     const float iso = V.binary ? 0.5f : V.iso;
     const int u8_thr = V.u8_thr;
 
-    s_cnt[tid] = c_vertex_count[tid];
+    C.cnt[tid] = c_vertex_count[tid];
     if (tid == 0) {
-        for (int s = 0; s < kRingStages; s++) mbar_init(&s_bar[s], 1);
+        for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
         mbar_fence_init();
     }
     __syncthreads();
     if (tid == 0) {
         for (int k = 0; k < kRingStages && k < nbox; k++) {
-            mbar_arrive_expect_tx(&s_bar[k], STAGE_BYTES);
-            tma_load_3d(s_ring + k * STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &s_bar[k]);
+            mbar_arrive_expect_tx(&C.bar[k], G::STAGE_BYTES);
+            tma_load_3d(s_ring + k * G::STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &C.bar[k]);
         }
     }
-    // cells of this lane's row inside the grid (masked codes are 0, shadergen.cpp:112-125)
-    const int xv = V.cells[0] - x0;
-    const uint32_t xmask = xv >= 32 ? 0xffffffffu : ((1u << xv) - 1u);
-    const uint32_t vmask = (y0 + lane < V.cells[1]) ? xmask : 0u;
+    const uint32_t vmask = row_mask(V, x0, y0, lane);
 
     bool timed_out = false;
     int k = 0;
@@ -248,64 +322,116 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         const int lb = k * kLayersPerBox;
         const int nl = min(kLayersPerBox, nlayers - lb);
         // every warp waits on the box's mbarrier (suspended in hardware, not spinning)
-        if (!mbar_wait_bounded(&s_bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout)) timed_out = true;
-        const T* st = reinterpret_cast<const T*>(s_ring + s * STAGE_STRIDE);
-#pragma unroll
-        for (int l = 0; l < kLayersPerBox; l++) {
-            if (l < nl && !timed_out) {
-                // warp w: rows 4w .. 4w+3 (one ballot per row, one 16-byte store)
-                const T* layer = st + l * LAYER;
-                const int buf = (lb + l) & 15;
-                const T* row = layer + 4 * warp * BXE + lane;
-                const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(row[0], iso, u8_thr));
-                const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(row[BXE], iso, u8_thr));
-                const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(row[2 * BXE], iso, u8_thr));
-                const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(row[3 * BXE], iso, u8_thr));
-                if (lane == 0) *reinterpret_cast<uint4*>(&s_rows[buf][4 * warp]) = make_uint4(b0, b1, b2, b3);
-                if (warp == ((lb + l + 3) & 7)) {  // row 32 and column x0+32 (a warp not classifying)
-                    const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(layer[32 * BXE + lane], iso, u8_thr));
-                    const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(layer[lane * BXE + 32], iso, u8_thr));
-                    const bool corner = below<FT>(layer[32 * BXE + 32], iso, u8_thr);
-                    if (lane == 0) {
-                        s_rows[buf][32] = r32;
-                        s_col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
-                    }
-                }
-            }
-        }
+        if (!mbar_wait_bounded(&C.bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout)) timed_out = true;
+        if (!timed_out)
+            convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl, (uint32_t)lb,
+                            iso, u8_thr, warp, lane, C);
         // the only CTA barrier of a box: stage s consumed, bit rows of layers
         // lb .. lb+nl-1 ready, and a uniform decision on a timed-out wait
         if (__syncthreads_or(timed_out)) break;
         if (tid == 0 && k + kRingStages < nbox) {
-            mbar_arrive_expect_tx(&s_bar[s], STAGE_BYTES);
-            tma_load_3d(s_ring + s * STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox, &s_bar[s]);
+            mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
+            tma_load_3d(s_ring + s * G::STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox,
+                        &C.bar[s]);
         }
-        // slices whose upper layer arrived in this box, warp (slice mod 8) each,
-        // so the work rotates over the warps from box to box.  A warp may still
-        // classify box k while others convert box k+1: row buffers (layer mod 16)
-        // of box k are not rewritten before box k+4.
-        const int sl = lb - 1 + ((warp - (lb - 1)) & 7);  // the slice of this warp, if any
-        if (sl >= 0 && sl <= lb + nl - 2) {
-            const int bb = sl & 15, bt = (sl + 1) & 15;
-            classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, s_rows[bb], s_col[bb], s_rows[bt], s_col[bt],
-                                s_cnt);
-        }
+        classify_box_slices(V, z0, fx, fy, lb, nl, 0u, warp, lane, vmask, C);
     }
     if (timed_out) {
         // drain the boxes still in flight (bounded) before the CTA exits
         if (tid == 0) {
             for (int l = k; l < nbox && l < k + kRingStages; l++)
-                mbar_wait_bounded(&s_bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, kWaitLimitNs, nullptr, 0u);
+                mbar_wait_bounded(&C.bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, kWaitLimitNs, nullptr,
+                                  0u);
             atomicOr(&V.ctrl->status, kStatusTimeout);
         }
     }
 }
 
+// Persistent column classifier: CTA b takes columns b, b + gridDim.x, ...
+// (column = footprint (fx, fy) x one run of column_slices slices, numbered
+// footprint-fastest so that neighbouring CTAs share halo samples in L2).
+// Thread 0 streams the boxes of the CTA's columns back to back through the
+// ring, so the copy engine never idles between columns.
 template <int FT>
-__global__ void __launch_bounds__(kThreads) classify_column_tma(const __grid_constant__ CUtensorMap tmap,
-                                                                const __grid_constant__ Volume V) {
-    classify_column_body<FT>(&tmap, V, blockIdx.x, blockIdx.y, blockIdx.z);
+__global__ void __launch_bounds__(kThreads) classify_columns(const __grid_constant__ CUtensorMap tmap,
+                                                             const __grid_constant__ Volume V, int ncolumns) {
+    using G = ColumnGeom<FT>;
+    uint8_t* const s_ring = ring_base<FT>();
+    __shared__ __align__(16) ColumnSmem C;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int per_slab = V.nfx * V.nfy;
+    const int stride = (int)gridDim.x;
+    const float iso = V.binary ? 0.5f : V.iso;
+    const int u8_thr = V.u8_thr;
+    // column u -> footprint, first slice, layers (slices + 1)
+    auto column = [&](int u, int& fx, int& fy, int& z0, int& nlayers) {
+        const int zc = u / per_slab;
+        const int r = u - zc * per_slab;
+        fy = r / V.nfx;
+        fx = r - fy * V.nfx;
+        z0 = zc * V.column_slices;
+        nlayers = min(V.cells[2], z0 + V.column_slices) - z0 + 1;
+    };
+
+    C.cnt[tid] = c_vertex_count[tid];
+    if (tid == 0) {
+        for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    // producer state (thread 0): next box to issue = box pk of column pu
+    int pu = blockIdx.x, pk = 0;
+    uint32_t issued = 0;
+    auto issue_next = [&]() {
+        if (pu >= ncolumns) return;
+        int fx, fy, z0, nl;
+        column(pu, fx, fy, z0, nl);
+        const int s = (int)(issued % kRingStages);
+        mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
+        tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, fx * 32, fy * 32, z0 + pk * kLayersPerBox, &C.bar[s]);
+        issued++;
+        if (++pk * kLayersPerBox >= nl) {
+            pk = 0;
+            pu += stride;
+        }
+    };
+    if (tid == 0)
+        for (int i = 0; i < kRingStages; i++) issue_next();
+
+    bool timed_out = false;
+    uint32_t pos = 0;  // running box position (ring slot, phase, row-buffer index)
+    for (int u = blockIdx.x; u < ncolumns && !timed_out; u += stride) {
+        int fx, fy, z0, nlayers;
+        column(u, fx, fy, z0, nlayers);
+        const int nbox = (nlayers + kLayersPerBox - 1) / kLayersPerBox;
+        const uint32_t vmask = row_mask(V, fx * 32, fy * 32, lane);
+        const uint32_t glu = pos * kLayersPerBox;
+        for (int k = 0; k < nbox; k++, pos++) {
+            const int s = (int)(pos % kRingStages);
+            const uint32_t parity = (pos / kRingStages) & 1u;
+            const int lb = k * kLayersPerBox;
+            const int nl = min(kLayersPerBox, nlayers - lb);
+            const bool ok = mbar_wait_bounded(&C.bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout);
+            if (ok)
+                convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl,
+                                pos * kLayersPerBox, iso, u8_thr, warp, lane, C);
+            // the only CTA barrier of a box (uniform decision on a timed-out wait)
+            if (__syncthreads_or(!ok)) {
+                timed_out = true;
+                break;
+            }
+            if (tid == 0) issue_next();  // refill stage s
+            classify_box_slices(V, z0, fx, fy, lb, nl, glu, warp, lane, vmask, C);
+        }
+    }
+    if (timed_out && tid == 0) {
+        // drain the boxes still in flight (bounded) before the CTA exits
+        for (uint32_t p = pos; p < issued; p++)
+            mbar_wait_bounded(&C.bar[p % kRingStages], (p / kRingStages) & 1u, kWaitLimitNs, nullptr, 0u);
+        atomicOr(&V.ctrl->status, kStatusTimeout);
+    }
 }
+
 
 // ---------------------------------------------------------------------------
 // Generic classification: CTA = one 32x32 block of the virtual cell grid,
@@ -584,16 +710,33 @@ __global__ void __launch_bounds__(kThreads) reduce_batch(const __grid_constant__
 constexpr int kRingBytesF32 = kRingStages * ((36 * 33 * 4 * kLayersPerBox + 127) & ~127) + 128;
 constexpr int kRingBytesU8 = kRingStages * ((48 * 33 * kLayersPerBox + 127) & ~127) + 128;
 
+// Resident column-classifier CTAs per SM (shared-memory bound).
+static int column_ctas_per_sm() {
+    static int n = 0;
+    if (n == 0) {
+        column_smem_ok();
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, classify_columns<kFieldF32>, kThreads,
+                                                          kRingBytesF32) !=
+                cudaSuccess ||
+            n < 1)
+            n = 1;
+    }
+    return n;
+}
+
 cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ctas, cudaStream_t st) {
     if (V.column_layout && tmap) {
         const int nz = (V.cells[2] + V.column_slices - 1) / V.column_slices;
-        const dim3 grid(V.nfx, V.nfy, nz);
+        const int ncolumns = V.nfx * V.nfy * nz;
+        // persistent: every resident CTA slot (max_ctas = 16 per SM)
+        const int slots = (max_ctas / 16) * column_ctas_per_sm();
+        const int grid = ncolumns < slots ? ncolumns : slots;
         if (V.ftype == kFieldF32)
-            classify_column_tma<kFieldF32><<<grid, kThreads, kRingBytesF32, st>>>(*tmap, V);
+            classify_columns<kFieldF32><<<grid, kThreads, kRingBytesF32, st>>>(*tmap, V, ncolumns);
         else if (V.ftype == kFieldU8)
-            classify_column_tma<kFieldU8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V);
+            classify_columns<kFieldU8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V, ncolumns);
         else
-            classify_column_tma<kFieldUNorm8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V);
+            classify_columns<kFieldUNorm8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V, ncolumns);
     } else {
         const long long nb = V.nblocks;
         const int grid = (int)(nb < (long long)max_ctas ? nb : (long long)max_ctas);
@@ -648,9 +791,9 @@ cudaError_t launch_reduce_batch(const BatchDev& B, unsigned int chunks, cudaStre
 bool column_smem_ok() {
     static int configured = 0;
     if (!configured) {
-        cudaFuncSetAttribute(classify_column_tma<kFieldF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesF32);
-        cudaFuncSetAttribute(classify_column_tma<kFieldU8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesU8);
-        cudaFuncSetAttribute(classify_column_tma<kFieldUNorm8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(classify_columns<kFieldF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesF32);
+        cudaFuncSetAttribute(classify_columns<kFieldU8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesU8);
+        cudaFuncSetAttribute(classify_columns<kFieldUNorm8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kRingBytesU8);
         cudaFuncSetAttribute(classify_batch_tma<kFieldF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesF32);
         cudaFuncSetAttribute(classify_batch_tma<kFieldU8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytesU8);
