@@ -42,12 +42,12 @@ WORKLOAD = ("cayley_512: FP32 512^3 lattice, Cayley cubic 16xyz+4(x^2+y^2+z^2)-1
             "iso 0, central-difference normals, float4 position+normal streams")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (read + write) of one build (classify_column_tma + reduce_levels)
+# DRAM bytes (read + write) of one build (classify_columns + reduce_levels)
 # per field byte, from ncu captures on the 384^3 Cayley field
-# (profiles/classify_column_tma_cayley384.txt, profiles/reduce_levels_cayley384.txt):
-# (226,523,136 + 11,095,296 + 1,067,264) / 226,492,416.  Traffic grows with
+# (profiles/classify_columns_cayley384.txt, profiles/reduce_levels_cayley384.txt):
+# (226,560,000 + 8,833,024 + 1,067,264) / 226,492,416.  Traffic grows with
 # the field, so the 512^3 figure is this ratio times the field bytes.
-BUILD_TRAFFIC_PER_FIELD_BYTE = (226523136 + 11095296 + 1067264) / 226492416
+BUILD_TRAFFIC_PER_FIELD_BYTE = (226560000 + 8833024 + 1067264) / 226492416
 
 
 def hbm_peak():
@@ -388,7 +388,7 @@ def run_hpmc(args, rank, world, local_rank):
     trav_avg = statistics.mean(trav_ms)
     out_bytes = 32 * nverts
     alg_bytes = field_bytes + out_bytes
-    roof = {"kernel": "build = classify_column_tma + reduce_levels (classify dominates)",
+    roof = {"kernel": "build = classify_columns + reduce_levels (classify dominates)",
             "bound": "hbm", "achieved": field_bytes / (build_avg * 1e-3) / 1e9, "peak": peak,
             "unit": "GB/s", "frac": field_bytes / (build_avg * 1e-3) / 1e9 / peak,
             "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes,

@@ -97,5 +97,39 @@ def build(verbose_ptxas: bool = False) -> str:
     return LIB
 
 
+APPS_DIR = os.path.join(PKG, "apps")
+APPS_OUT = os.path.join(OUT_DIR, "apps")
+APPS = ["texture3d", "cayley", "metaballs", "transform_feedback"]
+
+
+def app_path(name: str) -> str:
+    return os.path.join(APPS_OUT, "hpmc_" + name)
+
+
+def build_apps() -> list[str]:
+    """Headless ports of the reference's apps (C++ callers of the C ABI),
+    linked against the library: ``_lib/apps/hpmc_<name>``."""
+    lib = build()
+    os.makedirs(APPS_OUT, exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    cuda = os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
+    out = []
+    for name in APPS:
+        src = os.path.join(APPS_DIR, name + ".cpp")
+        dst = app_path(name)
+        deps = [src, os.path.join(APPS_DIR, "app_common.hpp"), os.path.join(ROOT, "include", "hpmc.h"), lib]
+        if not os.path.exists(dst) or os.path.getmtime(dst) < max(os.path.getmtime(d) for d in deps):
+            cmd = [cxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(cuda, "include"),
+                   src, "-o", dst, "-L" + OUT_DIR, "-lhpmc_b200", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
+                   "-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"app build failed for {name}:\n{r.stdout}\n{r.stderr}")
+        out.append(dst)
+    return out
+
+
 if __name__ == "__main__":
     print(build(verbose_ptxas="-v" in sys.argv))
+    for a in build_apps():
+        print(a)

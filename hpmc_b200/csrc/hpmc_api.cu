@@ -21,6 +21,7 @@
 
 #include "hpmc.h"
 #include "hpmc_device.cuh"
+#include "hpmc_fetch.cuh"
 #include "hpmc_host.h"
 #include "hpmc_kernels.h"
 
@@ -126,8 +127,10 @@ int bind_field(HPMCHistoPyramid* h) {
         V.field = nullptr;
         V.row_pitch = V.slice_pitch = 0;
         V.functor = h->functor;
+        V.gradient = (h->gradient && hpmc::functor_has_gradient(h->functor.id)) ? 1 : 0;
         return HPMC_OK;
     }
+    V.gradient = 0;
     if (h->fmode != HPMCHistoPyramid::kArray || !h->field.ptr) return HPMC_ERR_NO_FIELD;
     const FieldDesc& f = h->field;
     const size_t es = elem_size(f.type);

@@ -83,6 +83,7 @@ struct Volume {
     int cells[3];
     float iso;
     int binary;
+    int gradient;            // functor field with analytic gradient normals (HPMC_fetchGrad)
     float scale[3];          // extent / cells
     double dscale[3];        // extent / cells in FP64 (geometry)
     // layout (init.cpp:72-149); all sizes are powers of two

@@ -23,23 +23,36 @@ enum FunctorId : int {
     kFunctorSpheres = 4,        // signed distance of a union of spheres; p = {n, (cx,cy,cz,r) x n}
 };
 
+// Functor arithmetic is written with round-to-nearest intrinsics in a fixed
+// order (no FMA contraction), so a host restatement in plain FP32 C with
+// contraction off gives bit-identical values -- and the same topology.
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+
 __device__ __forceinline__ float functor_value(const FunctorParams& F, float px, float py, float pz) {
     switch (F.id) {
         case kFunctorCayley: {
-            float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
-            return 1.0f - 16.0f * x * y * z - 4.0f * x * x - 4.0f * y * y - 4.0f * z * z;
+            const float x = fs(fm(2.0f, px), 1.0f), y = fs(fm(2.0f, py), 1.0f), z = fs(fm(2.0f, pz), 1.0f);
+            // 1 - 16xyz - 4x^2 - 4y^2 - 4z^2, left to right
+            float v = fs(1.0f, fm(fm(fm(16.0f, x), y), z));
+            v = fs(v, fm(fm(4.0f, x), x));
+            v = fs(v, fm(fm(4.0f, y), y));
+            return fs(v, fm(fm(4.0f, z), z));
         }
         case kFunctorMetaballs: {
-            int n = (int)F.p[0];
+            const int n = (int)F.p[0];
             float s = 0.0f;
             for (int i = 0; i < n; i++) {
-                float dx = px - F.p[1 + 4 * i], dy = py - F.p[2 + 4 * i], dz = pz - F.p[3 + 4 * i];
-                float r = F.p[4 + 4 * i];
-                s += (r * r) / (dx * dx + dy * dy + dz * dz);
+                const float dx = fs(px, F.p[1 + 4 * i]), dy = fs(py, F.p[2 + 4 * i]), dz = fs(pz, F.p[3 + 4 * i]);
+                const float r = F.p[4 + 4 * i];
+                s = fa(s, __fdiv_rn(fm(r, r), fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz))));
             }
             return s;
         }
         case kFunctorTwistMetaballs: {
+            // sin/cos: device and host libraries round differently, so this
+            // functor agrees with a host restatement only to a few ulps
             float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
             float twist = F.p[0];
             float rot1 = twist * z, rot2 = 0.7f * twist * y;
@@ -58,11 +71,11 @@ __device__ __forceinline__ float functor_value(const FunctorParams& F, float px,
             return s;
         }
         case kFunctorSpheres: {
-            int n = (int)F.p[0];
+            const int n = (int)F.p[0];
             float d = 3.0e38f;
             for (int i = 0; i < n; i++) {
-                float dx = px - F.p[1 + 4 * i], dy = py - F.p[2 + 4 * i], dz = pz - F.p[3 + 4 * i];
-                d = fminf(d, sqrtf(dx * dx + dy * dy + dz * dz) - F.p[4 + 4 * i]);
+                const float dx = fs(px, F.p[1 + 4 * i]), dy = fs(py, F.p[2 + 4 * i]), dz = fs(pz, F.p[3 + 4 * i]);
+                d = fminf(d, fs(__fsqrt_rn(fa(fa(fm(dx, dx), fm(dy, dy)), fm(dz, dz))), F.p[4 + 4 * i]));
             }
             return d;
         }
@@ -71,17 +84,28 @@ __device__ __forceinline__ float functor_value(const FunctorParams& F, float px,
     }
 }
 
-// Analytic gradient where the functor provides one (HPMC_fetchGrad).
+// Functors with an analytic gradient (HPMC_fetchGrad of the reference's
+// custom snippet, e.g. apps/cayley/cayley.cpp:85-93).
+__host__ __device__ __forceinline__ bool functor_has_gradient(int id) { return id == kFunctorCayley; }
+
+// The gradient in the snippet's own coordinates (cayley: with respect to
+// x = 2p - 1, as apps/cayley/cayley.cpp:90-92 returns it).
 __device__ __forceinline__ void functor_gradient(const FunctorParams& F, float px, float py, float pz,
                                                  float& gx, float& gy, float& gz) {
     if (F.id == kFunctorCayley) {
-        float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
-        gx = -16.0f * y * z - 8.0f * x;
-        gy = -16.0f * x * z - 8.0f * y;
-        gz = -16.0f * x * y - 8.0f * z;
+        const float x = fs(fm(2.0f, px), 1.0f), y = fs(fm(2.0f, py), 1.0f), z = fs(fm(2.0f, pz), 1.0f);
+        gx = fs(fm(fm(-16.0f, y), z), fm(8.0f, x));
+        gy = fs(fm(fm(-16.0f, x), z), fm(8.0f, y));
+        gz = fs(fm(fm(-16.0f, x), y), fm(8.0f, z));
     } else {
         gx = gy = gz = 0.0f;
     }
+}
+
+// Texel centre of lattice index i along an axis of `n` samples (the
+// reference's normalised coordinate, shadergen.cpp:257).
+__device__ __forceinline__ float texel_centre(int i, int n) {
+    return __fdiv_rn(fa((float)i, 0.5f), (float)n);
 }
 
 // uint8 -> float without the conversion pipe: exact for b < 2^23.
@@ -113,10 +137,8 @@ __device__ __forceinline__ float fetch_raw(const Volume& V, long long off) {
 template <int FT>
 __device__ __forceinline__ float fetch(const Volume& V, int x, int y, int z) {
     if constexpr (FT == kFieldFunctor) {
-        float px = ((float)x + 0.5f) / (float)V.lattice[0];
-        float py = ((float)y + 0.5f) / (float)V.lattice[1];
-        float pz = ((float)z + 0.5f) / (float)V.lattice[2];
-        return functor_value(V.functor, px, py, pz);
+        return functor_value(V.functor, texel_centre(x, V.lattice[0]), texel_centre(y, V.lattice[1]),
+                             texel_centre(z, V.lattice[2]));
     } else {
         x = min(max(x, 0), V.lattice[0] - 1);
         y = min(max(y, 0), V.lattice[1] - 1);

@@ -153,6 +153,28 @@ __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int a
         n[0] = binary_normal[0];
         n[1] = binary_normal[1];
         n[2] = binary_normal[2];
+    } else if (FT == kFieldFunctor && V.gradient) {
+        // analytic gradient (shadergen.cpp:539-551): t from the functor values
+        // at a and b; forward mode keeps the reference's n = iso - lerp(grad a,
+        // grad b, t), central mode gives -lerp(grad a, grad b, t)
+        const float pa[3] = {texel_centre(a[0], V.lattice[0]), texel_centre(a[1], V.lattice[1]),
+                             texel_centre(a[2], V.lattice[2])};
+        const int b[3] = {a[0] + (axis == 0), a[1] + (axis == 1), a[2] + (axis == 2)};
+        const float pb[3] = {texel_centre(b[0], V.lattice[0]), texel_centre(b[1], V.lattice[1]),
+                             texel_centre(b[2], V.lattice[2])};
+        const float va = functor_value(V.functor, pa[0], pa[1], pa[2]);
+        const float vb = functor_value(V.functor, pb[0], pb[1], pb[2]);
+        float ga[3], gb[3];
+        functor_gradient(V.functor, pa[0], pa[1], pa[2], ga[0], ga[1], ga[2]);
+        functor_gradient(V.functor, pb[0], pb[1], pb[2], gb[0], gb[1], gb[2]);
+        const float iso = V.iso;
+        const FF tf = ff_ratio_of_diffs(va, iso, va, vb);
+        t = tf.hi + tf.lo;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const float g = ff_lerp(FF{ga[i], 0.0f}, FF{gb[i], 0.0f}, tf);
+            n[i] = (MODE == kGeomCentral) ? -g : iso - g;
+        }
     } else {
         EdgeField F;
         gather_edge<FT, MODE == kGeomCentral>(V, a, axis, cx, cy, cz, F);

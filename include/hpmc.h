@@ -105,8 +105,10 @@ void HPMCsetFieldTexture3D(struct HPMCHistoPyramid* h, GLuint texture, GLboolean
  * device functor instead of carrying GLSL: "hpmc:cayley",
  * "hpmc:metaballs", "hpmc:twist_metaballs", "hpmc:spheres".  Any other text
  * sets HPMC_ERR_UNSUPPORTED and breaks the handle.  builder_texunit is
- * ignored.  gradient = GL_TRUE uses the functor's analytic gradient for
- * normals where it has one (cayley). */
+ * ignored.  gradient = GL_TRUE uses the functor's analytic gradient where it
+ * has one (cayley): t from the functor values at the edge ends and, as the
+ * reference computes it (shadergen.cpp:539-551), n = iso - lerp(grad a,
+ * grad b, t); with HPMC_NORMALS_CENTRAL, n = -lerp(grad a, grad b, t). */
 void HPMCsetFieldCustom(struct HPMCHistoPyramid* h, const char* shader_source, GLuint builder_texunit,
                         GLboolean gradient);
 

@@ -160,11 +160,81 @@ void oracle_tables(uint8_t* count, uint8_t* edge_index, float* edge_decode,
 /* ------------------------------------------------------------------------- */
 static inline long clampl(long v, long lo, long hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+/* Functor fields in plain FP32 (this file is compiled with contraction off),
+ * the operations in the same order as the device's, so that values agree bit
+ * for bit (sin/cos of the twisted metaballs excepted). */
+static float functor_value(const oracle_functor_t* F, float px, float py, float pz)
+{
+    switch (F->id) {
+    case 1: {
+        const float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        return 1.0f - 16.0f * x * y * z - 4.0f * x * x - 4.0f * y * y - 4.0f * z * z;
+    }
+    case 2: {
+        const int n = (int)F->p[0];
+        float s = 0.0f;
+        for (int i = 0; i < n; i++) {
+            const float dx = px - F->p[1 + 4 * i], dy = py - F->p[2 + 4 * i], dz = pz - F->p[3 + 4 * i];
+            const float r = F->p[4 + 4 * i];
+            s = s + (r * r) / (dx * dx + dy * dy + dz * dz);
+        }
+        return s;
+    }
+    case 3: {
+        float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        const float twist = F->p[0];
+        const float rot1 = twist * z, rot2 = 0.7f * twist * y;
+        const float c1 = cosf(rot1), s1 = sinf(rot1), c2 = cosf(rot2), s2 = sinf(rot2);
+        const float x1 = c1 * x + s1 * y, y1 = -s1 * x + c1 * y, z1 = z;
+        const float x2 = c2 * x1 + s2 * z1, y2 = y1, z2 = -s2 * x1 + c2 * z1;
+        x = 0.5f * x2 + 0.5f;
+        y = 0.5f * y2 + 0.5f;
+        z = 0.5f * z2 + 0.5f;
+        float s = 0.0f;
+        for (int i = 0; i < 8; i++) {
+            const float dx = x - F->p[1 + 3 * i], dy = y - F->p[2 + 3 * i], dz = z - F->p[3 + 3 * i];
+            s += 0.05f / (dx * dx + dy * dy + dz * dz);
+        }
+        return s;
+    }
+    case 4: {
+        const int n = (int)F->p[0];
+        float d = 3.0e38f;
+        for (int i = 0; i < n; i++) {
+            const float dx = px - F->p[1 + 4 * i], dy = py - F->p[2 + 4 * i], dz = pz - F->p[3 + 4 * i];
+            d = fminf(d, sqrtf(dx * dx + dy * dy + dz * dz) - F->p[4 + 4 * i]);
+        }
+        return d;
+    }
+    default:
+        return 0.0f;
+    }
+}
+
+/* HPMC_fetchGrad of the cayley snippet (apps/cayley/cayley.cpp:85-93). */
+static void functor_gradient(const oracle_functor_t* F, float px, float py, float pz, float g[3])
+{
+    if (F->id == 1) {
+        const float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        g[0] = -16.0f * y * z - 8.0f * x;
+        g[1] = -16.0f * x * z - 8.0f * y;
+        g[2] = -16.0f * x * y - 8.0f * z;
+    } else {
+        g[0] = g[1] = g[2] = 0.0f;
+    }
+}
+
+static inline float texel_centre(long i, int n) { return ((float)i + 0.5f) / (float)n; }
+
 /* GL_CLAMP + NEAREST (apps/texture3d/texture3d.cpp:135-139): clamp to edge.
- * uint8 fetch: U8 is float(b); UNORM8 is b/255 as a GL_ALPHA texture reads. */
+ * uint8 fetch: U8 is float(b); UNORM8 is b/255 as a GL_ALPHA texture reads.
+ * Functors are evaluated at the texel centre, unclamped (shadergen.cpp:270-279). */
 static inline float sample_f(const void* field, int type, const oracle_layout_t* L,
                              size_t rp, size_t sp, long x, long y, long z)
 {
+    if (type == ORACLE_FUNCTOR)
+        return functor_value((const oracle_functor_t*)field, texel_centre(x, L->lattice[0]),
+                             texel_centre(y, L->lattice[1]), texel_centre(z, L->lattice[2]));
     x = clampl(x, 0, L->lattice[0] - 1);
     y = clampl(y, 0, L->lattice[1] - 1);
     z = clampl(z, 0, L->lattice[2] - 1);
@@ -394,6 +464,22 @@ void oracle_geometry(const void* field, int type, const oracle_layout_t* L, size
             for (int i = 0; i < 3; i++) {
                 float fr = en[i] - floorf(en[i]);
                 nn[i] = 2.0 * (double)fr - 1.0;
+            }
+        } else if (normal_mode >= ORACLE_NORMALS_GRADIENT && type == ORACLE_FUNCTOR) {
+            const oracle_functor_t* F = (const oracle_functor_t*)field;
+            const float pa[3] = {texel_centre(a[0], L->lattice[0]), texel_centre(a[1], L->lattice[1]),
+                                 texel_centre(a[2], L->lattice[2])};
+            const float pb[3] = {texel_centre(b[0], L->lattice[0]), texel_centre(b[1], L->lattice[1]),
+                                 texel_centre(b[2], L->lattice[2])};
+            const double va = functor_value(F, pa[0], pa[1], pa[2]);
+            const double vb = functor_value(F, pb[0], pb[1], pb[2]);
+            float ga[3], gb[3];
+            functor_gradient(F, pa[0], pa[1], pa[2], ga);
+            functor_gradient(F, pb[0], pb[1], pb[2], gb);
+            t = (va - thr) / (va - vb);
+            for (int i = 0; i < 3; i++) {
+                const double g = (1.0 - t) * ga[i] + t * gb[i];
+                nn[i] = normal_mode == ORACLE_NORMALS_GRADIENT ? thr - g : -g;
             }
         } else {
             double va = oracle_sample(field, type, L, rp, sp, a[0], a[1], a[2]);

@@ -18,8 +18,10 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REF_DIR = os.path.join(_HERE, "_ref")
 
-F32, U8, UNORM8, F64 = 0, 1, 2, 3  # F64: geometry and adjoint only
+F32, U8, UNORM8, F64, FUNCTOR = 0, 1, 2, 3, 4  # F64: geometry and adjoint only
 NORMALS_FORWARD, NORMALS_CENTRAL = 0, 1
+# analytic-gradient normals of a functor field: the reference's iso - lerp(grad), or -lerp(grad)
+NORMALS_GRADIENT, NORMALS_GRADIENT_CENTRAL = 2, 3
 
 
 def build(hpmc_src: str | None = None) -> None:
@@ -124,6 +126,35 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
+class _FunctorParams(C.Structure):
+    _fields_ = [("id", C.c_int), ("count", C.c_int), ("p", C.c_float * 136)]
+
+
+class Functor:
+    """A field functor on a lattice of `shape` (z, y, x): the oracle's form of
+    HPMCsetFieldCustom + HPMCsetBuilderUniforms (hpiface.cpp:187-222)."""
+
+    IDS = {"hpmc:cayley": 1, "hpmc:metaballs": 2, "hpmc:twist_metaballs": 3, "hpmc:spheres": 4}
+
+    def __init__(self, name: str, params, shape):
+        self.name = name
+        self.shape = tuple(int(v) for v in shape)
+        self.params = [float(v) for v in params]
+        self.c = _FunctorParams()
+        self.c.id = self.IDS[name]
+        self.c.count = len(self.params)
+        for i, v in enumerate(self.params):
+            self.c.p[i] = v
+
+
+def _field(field, unorm=False):
+    """(pointer, type, contiguous field) of an array or a Functor."""
+    if isinstance(field, Functor):
+        return C.cast(C.pointer(field.c), C.c_void_p), FUNCTOR, field
+    field = np.ascontiguousarray(field)
+    return _ptr(field), _field_type(field, unorm), field
+
+
 def _to_layout(s: _Layout) -> Layout:
     return Layout(tuple(s.lattice), tuple(s.cells), tuple(s.tile), tuple(s.layout), s.size_l2, s.size)
 
@@ -200,13 +231,12 @@ def _field_type(field: np.ndarray, unorm: bool) -> int:
 
 def codes(field: np.ndarray, L: Layout, iso: float, binary=False, unorm=False) -> np.ndarray:
     """Per-cell MC codes, shape (cz, cy, cx). field is C-contiguous (fz, fy, fx)."""
-    field = np.ascontiguousarray(field)
+    fptr, ftype, field = _field(field, unorm)
     cx, cy, cz = L.cells
     out = np.zeros((cz, cy, cx), np.uint8)
     fx, fy, _ = L.lattice
     s = _struct(L)
-    lib().oracle_codes(_ptr(field), _field_type(field, unorm), C.byref(s), fx, fx * fy,
-                       float(iso), int(binary), _ptr(out))
+    lib().oracle_codes(fptr, ftype, C.byref(s), fx, fx * fy, float(iso), int(binary), _ptr(out))
     return out
 
 
@@ -245,7 +275,7 @@ def traverse(codes_arr, levels, L: Layout, v0: int, v1: int):
 
 def geometry(field, L: Layout, iso, cell, code, k, edge, *, binary=False,
              normal_mode=NORMALS_FORWARD, extent=(1.0, 1.0, 1.0), unorm=False):
-    field = np.ascontiguousarray(field)
+    fptr, ftype, field = _field(field, unorm)
     _, _, _, edn = tables()
     n = len(edge)
     t = np.zeros(n, np.float64)
@@ -254,7 +284,7 @@ def geometry(field, L: Layout, iso, cell, code, k, edge, *, binary=False,
     fx, fy, _ = L.lattice
     s = _struct(L)
     ext = (C.c_float * 3)(*extent)
-    lib().oracle_geometry(_ptr(field), _field_type(field, unorm), C.byref(s), fx, fx * fy,
+    lib().oracle_geometry(fptr, ftype, C.byref(s), fx, fx * fy,
                           float(iso), int(binary), int(normal_mode), ext,
                           _ptr(np.ascontiguousarray(edn.reshape(-1))), n,
                           _ptr(np.ascontiguousarray(cell)), _ptr(np.ascontiguousarray(code)),

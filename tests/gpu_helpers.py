@@ -8,13 +8,17 @@ EPS32 = np.finfo(np.float32).eps
 
 
 def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=False, unorm=False,
-            normals=0, capture_codes=True, pitch_pad=0, tensor=None):
-    """Build + count + extract through the C ABI.  Returns a dict of numpy arrays."""
+            normals=0, capture_codes=True, pitch_pad=0, tensor=None, gradient=False):
+    """Build + count + extract through the C ABI.  Returns a dict of numpy arrays.
+    `field` is a numpy array or an oracle Functor (registered device functor)."""
     import torch
 
     dev = torch.device("cuda:0")
     fz, fy, fx = field.shape
-    if tensor is None:
+    functor = hasattr(field, "params")
+    if functor:
+        pass
+    elif tensor is None:
         if pitch_pad:
             big = torch.zeros((fz, fy, fx + pitch_pad), dtype=torch.from_numpy(field).dtype, device=dev)
             big[:, :, :fx] = torch.from_numpy(field).to(dev)
@@ -24,7 +28,14 @@ def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=Fals
     c = hpmc.default_constants()
     hp = hpmc.HistoPyramid(c)
     hp.set_stream(torch.cuda.current_stream())
-    hp.set_field_device(tensor, unorm=unorm)
+    if functor:
+        hp.set_lattice_size(fx, fy, fz)
+        hp.set_field_custom(field.name, gradient=gradient)
+        assert hp.builder_program() != 0
+        if field.params:
+            hp.set_builder_uniforms(field.params)
+    else:
+        hp.set_field_device(tensor, unorm=unorm)
     if cells is not None:
         hp.set_grid_size(*cells)
     hp.set_grid_extent(*extent)
