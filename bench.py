@@ -171,16 +171,21 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, dev, stream):
+def run_batched(args, dev, stream, rank=0, world=1):
     """64 uneven FP32 metaball volumes: one CUDA-graph replay of the batched
     extractor vs the plain per-volume loop through the handle API (build,
-    acquire count, extract), both on the same stream, CUDA events."""
+    acquire count, extract), both on the same stream, CUDA events.  With N
+    ranks each takes its share of the 64 volumes (greedy split by cells) and
+    the time is the maximum over the ranks."""
     import torch
+    import torch.distributed as dist
 
     import hpmc_b200 as H
-    from hpmc_b200 import datasets
+    from hpmc_b200 import datasets, multi
 
-    vols = datasets.batch_64()
+    all_vols = datasets.batch_64()
+    share = multi.split_volumes([f.size for f, _ in all_vols], world)[rank]
+    vols = [all_vols[i] for i in share]
     tensors = [torch.from_numpy(f).to(dev) for f, _ in vols]
     isos = [iso for _, iso in vols]
     cells = sum((f.shape[0] - 1) * (f.shape[1] - 1) * (f.shape[2] - 1) for f, _ in vols)
@@ -217,12 +222,14 @@ def run_batched(args, dev, stream):
         for _ in range(3):
             plain()
         stream.synchronize()
+        if world > 1:
+            dist.barrier()
         e0.record(stream)
         for _ in range(steps):
             plain()
         e1.record(stream)
         stream.synchronize()
-    plain_ms = e0.elapsed_time(e1) / steps
+    plain_ms = multi.max_over_ranks(e0.elapsed_time(e1) / steps, device=dev)
 
     b = H.Batch(tensors, isos, normals=H.NORMALS_CENTRAL)
     pos = torch.empty((total, 4), dtype=torch.float32, device=dev)
@@ -232,12 +239,14 @@ def run_batched(args, dev, stream):
         for _ in range(3):
             b.extract(pos, nrm, total, stream=stream)
         stream.synchronize()
+        if world > 1:
+            dist.barrier()
         e0.record(stream)
         for _ in range(steps):
             b.extract(pos, nrm, total, stream=stream)
         e1.record(stream)
         stream.synchronize()
-    batched_ms = e0.elapsed_time(e1) / steps
+    batched_ms = multi.max_over_ranks(e0.elapsed_time(e1) / steps, device=dev)
     offs = b.offsets()
     assert offs[-1] == total, (offs[-1], total)
     for th in ths:
@@ -245,12 +254,15 @@ def run_batched(args, dev, stream):
     for hp in hps:
         hp.close()
     b.close()
+    nall = len(all_vols)
+    cells_all = sum((f.shape[0] - 1) * (f.shape[1] - 1) * (f.shape[2] - 1) for f, _ in all_vols)
     return {"workload": "batch_64: 64 FP32 volumes, edges log-uniform [32,192] (x4), 4-32 metaballs, iso U[0.8,1.5], "
                         "central normals",
-            "volumes": len(vols), "cells": cells, "field_bytes": field_bytes, "vertices": total,
+            "volumes": nall, "cells": cells_all, "field_bytes": sum(f.nbytes for f, _ in all_vols),
+            "vertices": int(multi.sum_over_ranks(total, device=dev)), "ranks": world,
             "plain_ms": plain_ms, "batched_ms": batched_ms,
-            "plain_vols_per_s": len(vols) / (plain_ms * 1e-3), "batched_vols_per_s": len(vols) / (batched_ms * 1e-3),
-            "speedup": plain_ms / batched_ms, "batched_gcells_per_s": cells / (batched_ms * 1e-3) / 1e9,
+            "plain_vols_per_s": nall / (plain_ms * 1e-3), "batched_vols_per_s": nall / (batched_ms * 1e-3),
+            "speedup": plain_ms / batched_ms, "batched_gcells_per_s": cells_all / (batched_ms * 1e-3) / 1e9,
             "tuning": {"column_slices": tuning[0], "traverse_ctas_per_sm": tuning[1], "rounds": tuning[2]},
             "graph": True, "steps": steps}
 
@@ -317,7 +329,7 @@ def run_hpmc(args, rank, world, local_rank):
     import torch
 
     import hpmc_b200 as H
-    from hpmc_b200 import datasets
+    from hpmc_b200 import datasets, multi
 
     dev = torch.device(f"cuda:{local_rank}")
     torch.cuda.set_device(dev)
@@ -376,10 +388,7 @@ def run_hpmc(args, rank, world, local_rank):
     total_ms = t_begin.elapsed_time(t_end)
     build_ms = [ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps)]
     trav_ms = [ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps)]
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = multi.max_over_ranks(total_ms, device=dev)
     ms_per_step = total_ms / args.steps
     value = cells * world * args.steps / (total_ms * 1e-3) / 1e9
 
@@ -432,7 +441,7 @@ def run_hpmc(args, rank, world, local_rank):
 
     batched = None
     if not args.no_batch:
-        batched = run_batched(args, dev, stream)
+        batched = run_batched(args, dev, stream, rank, world)
     adjoint = None
     if not args.no_adjoint:
         adjoint = run_adjoint(args, dev, stream)
