@@ -257,6 +257,14 @@ struct EdgeGeom {
     int edge;
 };
 
+// Rounds of 32 vertices per work item: as many as possible (every item
+// starts with a descent to its first block) while every warp of the grid
+// still gets about two items; at most kMaxTraverseRounds.
+__device__ __forceinline__ uint32_t item_rounds(uint32_t N, uint32_t ctas) {
+    const uint32_t r = N / (32u * 2u * ctas * (uint32_t)kWarps);
+    return r < 1u ? 1u : (r > (uint32_t)kMaxTraverseRounds ? (uint32_t)kMaxTraverseRounds : r);
+}
+
 // Dynamic work queue over vertex chunks (balances the persistent grid):
 // lane 0 takes the next chunk for its warp.
 __device__ __forceinline__ uint32_t next_chunk(const Volume& V, int lane) {
@@ -323,13 +331,14 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
         if (total > O.capacity) atomicOr(&V.ctrl->status, kStatusCapacity);
         V.ctrl->written = N;
     }
-    constexpr uint32_t VW = 32u * kTraverseRounds;
+    const uint32_t rounds = item_rounds(N, gridDim.x);
+    const uint32_t VW = 32u * rounds;
     const uint32_t nchunks = (N + VW - 1) / VW;
     WarpBlock B;
     B.have = false;
     for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
-        for (int r = 0; r < kTraverseRounds; r++) {
+        for (uint32_t r = 0; r < rounds; r++) {
             const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
@@ -385,13 +394,14 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
     const unsigned long long total = V.ctrl->total;
     const uint32_t N = (uint32_t)(total < A.count ? total : A.count);
     const float iso = V.iso;
-    constexpr uint32_t VW = 32u * kTraverseRounds;
+    const uint32_t rounds = item_rounds(N, gridDim.x);
+    const uint32_t VW = 32u * rounds;
     const uint32_t nchunks = (N + VW - 1) / VW;
     WarpBlock B;
     B.have = false;
     for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
-        for (int r = 0; r < kTraverseRounds; r++) {
+        for (uint32_t r = 0; r < rounds; r++) {
             const uint32_t v = chunk * VW + 32u * r + lane;
             const bool act = v < N;
             if (!__any_sync(0xffffffffu, act)) break;
