@@ -21,11 +21,10 @@ constexpr int kColumnSliceChoices[4] = {63, 31, 15, 7};
 // Traversal: top pyramid entries cached in shared memory per CTA
 // (levels with <= 1024 entries: 1 + 4 + ... + 1024, each padded to 4).
 constexpr int kTopCacheEntries = 1368;
-// Vertices per warp work item (R rounds of 32): the host's grid sizing and
-// the batched traversal's default use kTraverseRounds; the single-volume
-// traversal picks up to kMaxTraverseRounds from the vertex count.
+// Vertices per warp work item (R rounds of 32) of the batched traversal (its
+// default; the autotuner chooses) and of the host's grid sizing; the
+// single-volume traversal gives each warp one contiguous range instead.
 constexpr int kTraverseRounds = 8;
-constexpr int kMaxTraverseRounds = 12;
 
 // Bounded waits: an mbarrier poll gives up after this long (a TMA box lands
 // in microseconds; only a fault in the copy path gets near it).

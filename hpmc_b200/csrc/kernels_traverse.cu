@@ -257,12 +257,16 @@ struct EdgeGeom {
     int edge;
 };
 
-// Rounds of 32 vertices per work item: as many as possible (every item
-// starts with a descent to its first block) while every warp of the grid
-// still gets about two items; at most kMaxTraverseRounds.
+// Rounds of 32 vertices per work item: one item per warp of the (resident,
+// persistent) grid, i.e. a contiguous vertex range per warp.  Every item
+// starts with a descent through dependent loads of the upper levels; after
+// that the warp walks from block to block, so fewer, longer items are faster
+// (measured: one item per warp beats two or four per warp), and per-vertex
+// work is uniform enough that the ranges stay balanced.
 __device__ __forceinline__ uint32_t item_rounds(uint32_t N, uint32_t ctas) {
-    const uint32_t r = N / (32u * 2u * ctas * (uint32_t)kWarps);
-    return r < 1u ? 1u : (r > (uint32_t)kMaxTraverseRounds ? (uint32_t)kMaxTraverseRounds : r);
+    const uint32_t warps = ctas * (uint32_t)kWarps;
+    const uint32_t r = (N + 32u * warps - 1u) / (32u * warps);
+    return r < 1u ? 1u : r;
 }
 
 // Dynamic work queue over vertex chunks (balances the persistent grid):
