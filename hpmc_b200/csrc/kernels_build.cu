@@ -11,6 +11,7 @@
 //   top readback (buildpass.cpp:161-168)-> Ctrl::total in device memory
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstdint>
 
 #include "hpmc_batch.cuh"
@@ -214,11 +215,14 @@ struct ColumnGeom {
 };
 
 struct ColumnSmem {
+    // 16-byte aligned: warps store 4 rows at a time (uint4), whatever the
+    // number of ring stages before it
+    alignas(16) uint32_t rows[kRowBuffers][36];  // bit x = sample (x0 + x, y0 + r) below iso; [32] = row 32
+    uint64_t col[kRowBuffers];                   // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
     uint64_t bar[kRingStages];
-    uint32_t rows[kRowBuffers][36];  // bit x = sample (x0 + x, y0 + r) below iso; [32] = row 32
-    uint64_t col[kRowBuffers];       // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
     uint8_t cnt[256];
 };
+static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4 row stores need 16-byte alignment");
 
 // Bit rows of the nl layers of one box (stage st), layer l stored at
 // running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
