@@ -52,17 +52,25 @@ def translate(text: str) -> str:
 
 
 _DRIVER = r"""
+#include <omp.h>
 extern "C" int glsl_run(const float* field, int fx, int fy, int fz, float iso, int size, int size_l2,
                         const float* count_rgba, const float* edge_rgba, float* mips, int max_vertices,
-                        float* pos, float* nrm) {
+                        float* pos, float* nrm, int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
     // --- base level (buildpass.cpp:62-92): one fragment per texel, texcoord at its centre
     std::vector<std::vector<float>> mip(size_l2 + 1);
     mip[0].assign((size_t)size * size * 4, 0.f);
-    sh_base::HPMC_scalarfield.alpha = field;
-    sh_base::HPMC_scalarfield.nx = fx; sh_base::HPMC_scalarfield.ny = fy; sh_base::HPMC_scalarfield.nz = fz;
-    sh_base::HPMC_vertex_count.rgba = count_rgba; sh_base::HPMC_vertex_count.n = 256;
-    sh_base::HPMC_threshold = iso;
-    for (int j = 0; j < size; j++)
+    sampler3D field_tex;
+    field_tex.alpha = field; field_tex.nx = fx; field_tex.ny = fy; field_tex.nz = fz;
+    sampler1D count_tex;
+    count_tex.rgba = count_rgba; count_tex.n = 256;
+#pragma omp parallel
+    {
+        sh_base::HPMC_scalarfield = field_tex;  // uniforms: once per thread
+        sh_base::HPMC_vertex_count = count_tex;
+        sh_base::HPMC_threshold = iso;
+#pragma omp for schedule(static)
+    for (int j = 0; j < size; j++) {
         for (int i = 0; i < size; i++) {
             sh_base::gl_TexCoord[0] = vec4((i + 0.5f) / (float)size, (j + 0.5f) / (float)size, 0.f, 1.f);
             sh_base::shader_main();
@@ -70,50 +78,62 @@ extern "C" int glsl_run(const float* field, int fx, int fy, int fz, float iso, i
             t[0] = sh_base::gl_FragColor.x; t[1] = sh_base::gl_FragColor.y;
             t[2] = sh_base::gl_FragColor.z; t[3] = sh_base::gl_FragColor.w;
         }
+    }
+    }
     // --- reductions (buildpass.cpp:104-159): first with the floor filter
-    sampler2D hp;
     for (int m = 1; m <= size_l2; m++) {
         const int w = size >> m;
         mip[m].assign((size_t)w * w * 4, 0.f);
-        hp.levels.clear(); hp.w.clear(); hp.h.clear();
+        sampler2D hp;
         for (int l = 0; l < m; l++) { hp.levels.push_back(mip[l].data()); hp.w.push_back(size >> l); hp.h.push_back(size >> l); }
-        for (int j = 0; j < w; j++)
+#pragma omp parallel
+        {
+            sh_first::HPMC_histopyramid = hp; sh_first::HPMC_src_level = 0;
+            sh_upper::HPMC_histopyramid = hp; sh_upper::HPMC_src_level = m - 1;
+#pragma omp for schedule(static)
+        for (int j = 0; j < w; j++) {
             for (int i = 0; i < w; i++) {
                 vec4 c;
                 if (m == 1) {
-                    sh_first::HPMC_histopyramid = hp; sh_first::HPMC_src_level = 0;
                     sh_first::gl_FragCoord = vec4(i + 0.5f, j + 0.5f, 0.f, 1.f);
                     sh_first::shader_main(); c = sh_first::gl_FragColor;
                 } else {
-                    sh_upper::HPMC_histopyramid = hp; sh_upper::HPMC_src_level = m - 1;
                     sh_upper::gl_FragCoord = vec4(i + 0.5f, j + 0.5f, 0.f, 1.f);
                     sh_upper::shader_main(); c = sh_upper::gl_FragColor;
                 }
                 float* t = &mip[m][4 * ((size_t)j * w + i)];
                 t[0] = c.x; t[1] = c.y; t[2] = c.z; t[3] = c.w;
             }
+        }
+        }
     }
     size_t off = 0;
-    for (int m = 0; m <= size_l2; m++) {
-        std::copy(mip[m].begin(), mip[m].end(), mips + off);
-        off += mip[m].size();
-    }
+    if (mips)
+        for (int m = 0; m <= size_l2; m++) {
+            std::copy(mip[m].begin(), mip[m].end(), mips + off);
+            off += mip[m].size();
+        }
     // --- count (hpiface.cpp:323-327)
     const float* top = mip[size_l2].data();
     const int N = (int)(std::floor(top[0]) + std::floor(top[1]) + std::floor(top[2]) + std::floor(top[3]));
     // --- extraction (triface.cpp:423-428): extractVertex per vertex id
-    hp.levels.clear(); hp.w.clear(); hp.h.clear();
+    sampler2D hp;
     for (int l = 0; l <= size_l2; l++) { hp.levels.push_back(mip[l].data()); hp.w.push_back(size >> l); hp.h.push_back(size >> l); }
     sampler2D et; et.levels.push_back(edge_rgba); et.w.push_back(16); et.h.push_back(256);
-    sh_ext::HPMC_histopyramid = hp; sh_ext::HPMC_edge_table = et;
-    sh_ext::HPMC_scalarfield = sh_base::HPMC_scalarfield;
-    sh_ext::HPMC_threshold = iso; sh_ext::HPMC_key_offset = 0.f;
-    for (int v = 0; v < N && v < max_vertices; v++) {
+    const int nv = N < max_vertices ? N : max_vertices;
+#pragma omp parallel
+    {
+        sh_ext::HPMC_histopyramid = hp; sh_ext::HPMC_edge_table = et;
+        sh_ext::HPMC_scalarfield = field_tex;
+        sh_ext::HPMC_threshold = iso; sh_ext::HPMC_key_offset = 0.f;
+#pragma omp for schedule(static)
+    for (int v = 0; v < nv; v++) {
         sh_ext::gl_VertexID = v;
         vec3 p, n;
         sh_ext::extractVertex(p, n);
-        pos[3 * v] = p.x; pos[3 * v + 1] = p.y; pos[3 * v + 2] = p.z;
-        nrm[3 * v] = n.x; nrm[3 * v + 1] = n.y; nrm[3 * v + 2] = n.z;
+        pos[3 * (size_t)v] = p.x; pos[3 * (size_t)v + 1] = p.y; pos[3 * (size_t)v + 2] = p.z;
+        nrm[3 * (size_t)v] = n.x; nrm[3 * (size_t)v + 1] = n.y; nrm[3 * (size_t)v + 2] = n.z;
+    }
     }
     return N;
 }
@@ -125,13 +145,18 @@ def program(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
     g = lambda which: O.ref_glsl(which, lattice, cells, extent)  # noqa: E731
     defines, fetch = g(0), translate(g(1))
     parts = ['#include "glsl_emu.hpp"', "#include <algorithm>", "using namespace glsl;", translate(defines)]
-    parts.append("namespace sh_base {\nsampler3D HPMC_scalarfield; sampler1D HPMC_vertex_count; float HPMC_threshold;\n"
-                 "vec4 gl_FragColor; vec4 gl_TexCoord[1];\n" + fetch + translate(g(2)) + "}")
+    # uniforms and built-ins are per-thread: the harness runs fragments and
+    # vertices in parallel (OpenMP), one shader invocation per thread at a time
+    parts.append("namespace sh_base {\nthread_local sampler3D HPMC_scalarfield; thread_local sampler1D HPMC_vertex_count;\n"
+                 "thread_local float HPMC_threshold;\nthread_local vec4 gl_FragColor; thread_local vec4 gl_TexCoord[1];\n"
+                 + fetch + translate(g(2)) + "}")
     for ns, which in (("sh_first", 3), ("sh_upper", 4)):
-        parts.append(f"namespace {ns} {{\nsampler2D HPMC_histopyramid; int HPMC_src_level; vec2 HPMC_delta;\n"
-                     "vec4 gl_FragColor; vec4 gl_FragCoord;\n" + translate(g(which)) + "}")
-    parts.append("namespace sh_ext {\nsampler3D HPMC_scalarfield; sampler2D HPMC_histopyramid; sampler2D HPMC_edge_table;\n"
-                 "float HPMC_key_offset; float HPMC_threshold; int gl_VertexID;\n" + fetch + translate(g(5)) + "}")
+        parts.append(f"namespace {ns} {{\nthread_local sampler2D HPMC_histopyramid; thread_local int HPMC_src_level;\n"
+                     "thread_local vec2 HPMC_delta;\nthread_local vec4 gl_FragColor; thread_local vec4 gl_FragCoord;\n"
+                     + translate(g(which)) + "}")
+    parts.append("namespace sh_ext {\nthread_local sampler3D HPMC_scalarfield; thread_local sampler2D HPMC_histopyramid;\n"
+                 "thread_local sampler2D HPMC_edge_table; thread_local float HPMC_key_offset;\n"
+                 "thread_local float HPMC_threshold; thread_local int gl_VertexID;\n" + fetch + translate(g(5)) + "}")
     parts.append(_DRIVER)
     return "\n".join(parts)
 
@@ -147,18 +172,20 @@ def build(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
         with open(cpp, "w") as f:
             f.write(src)
         cxx = shutil.which("g++") or "/usr/bin/g++"
-        r = subprocess.run([cxx, "-O1", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-I" + HERE, cpp,
-                            "-o", so + ".tmp"], capture_output=True, text=True)
+        r = subprocess.run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared",
+                            "-I" + HERE, cpp, "-o", so + ".tmp"], capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"GLSL translation did not compile:\n{r.stderr[:4000]}")
         os.replace(so + ".tmp", so)
     return so
 
 
-def run(field: np.ndarray, iso: float, cells=None, extent=(1.0, 1.0, 1.0), max_vertices: int = 1 << 20):
+def run(field: np.ndarray, iso: float, cells=None, extent=(1.0, 1.0, 1.0), max_vertices: int = 1 << 20,
+        threads: int = 0, keep_levels: bool = True):
     """The reference's passes on a float field (z, y, x) as a float alpha
-    texture.  Returns (mip levels as (w, w, 4) arrays, vertex count,
-    positions (n, 3), normals (n, 3)), all FP32 as the shaders compute them."""
+    texture, on `threads` host threads (0: all).  Returns (mip levels as
+    (w, w, 4) arrays -- empty unless keep_levels --, vertex count, positions
+    (n, 3), normals (n, 3)), all FP32 as the shaders compute them."""
     fz, fy, fx = field.shape
     lattice = (fx, fy, fz)
     L = O.layout(lattice, cells)
@@ -169,17 +196,18 @@ def run(field: np.ndarray, iso: float, cells=None, extent=(1.0, 1.0, 1.0), max_v
     edge_rgba = np.ascontiguousarray(ed.reshape(256, 16, 4).astype(np.float32))
     size, l2 = L.size, L.size_l2
     mips_len = sum((size >> m) ** 2 * 4 for m in range(l2 + 1))
-    mips = np.zeros(mips_len, np.float32)
+    mips = np.zeros(mips_len if keep_levels else 1, np.float32)
     pos = np.zeros((max_vertices, 3), np.float32)
     nrm = np.zeros((max_vertices, 3), np.float32)
     f = np.ascontiguousarray(field, dtype=np.float32)
     fn = lib.glsl_run
     fn.restype = C.c_int
     p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
-    n = fn(p(f), fx, fy, fz, C.c_float(iso), size, l2, p(count_rgba), p(edge_rgba), p(mips), max_vertices, p(pos),
-           p(nrm))
+    threads = int(threads) if threads and threads > 0 else (os.cpu_count() or 1)
+    n = fn(p(f), fx, fy, fz, C.c_float(iso), size, l2, p(count_rgba), p(edge_rgba),
+           p(mips) if keep_levels else None, max_vertices, p(pos), p(nrm), threads)
     levels, off = [], 0
-    for m in range(l2 + 1):
+    for m in range(l2 + 1 if keep_levels else 0):
         w = size >> m
         levels.append(mips[off:off + w * w * 4].reshape(w, w, 4))
         off += w * w * 4
