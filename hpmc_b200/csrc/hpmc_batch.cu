@@ -31,7 +31,7 @@ namespace {
 constexpr uint32_t kMagicBatch = 0x48504231u;  // "HPB1"
 
 // Tuning choices (autotuner search space).
-constexpr int kRoundChoices[3] = {4, 8, 16};
+constexpr int kRoundChoices[5] = {4, 8, 16, 32, 64};
 constexpr int kTraverseCtaChoices[3] = {2, 3, 4};
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }

@@ -292,7 +292,7 @@ int HPMCbatchGetOffsets(struct HPMCBatch* b, unsigned long long* host_offsets);
 int HPMCbatchGetDeviceOffsets(struct HPMCBatch* b, const unsigned long long** device_offsets);
 /* Brick depth (slices per column CTA: 7, 15, 31, 63; 0 = automatic),
  * traversal CTAs per SM (0 = maximum) and rounds of 32 vertices per
- * traversal work item (0 = default). */
+ * traversal work item (1..64; 0 = default). */
 int HPMCbatchSetTuning(struct HPMCBatch* b, int column_slices, int traverse_ctas_per_sm, int rounds);
 int HPMCbatchGetTuning(struct HPMCBatch* b, int out[3]);
 /* Times every tuning choice on these outputs (graph replays, CUDA events)
