@@ -230,6 +230,18 @@ class TraversalHandle:
             raise HPMCError(st, "HPMCextractVerticesToBuffers")
         return int(n.value)
 
+    def extract_indexed(self, pos, nrm, indices, vertex_capacity: int | None = None,
+                        index_capacity: int | None = None):
+        """Welded output (HPMCextractVerticesIndexed): one vertex per crossed
+        edge in first-occurrence order, one index per soup vertex.  Returns
+        (unique vertices, indices); raises unless both fit."""
+        vcap = vertex_capacity if vertex_capacity is not None else (pos if pos is not None else nrm).shape[0]
+        icap = index_capacity if index_capacity is not None else indices.numel()
+        nv, ni = C.c_uint64(0), C.c_uint64(0)
+        _check(lib().HPMCextractVerticesIndexed(self.ptr, _ptr(pos), _ptr(nrm), int(vcap), _ptr(indices), int(icap),
+                                                C.byref(nv), C.byref(ni)), "HPMCextractVerticesIndexed")
+        return int(nv.value), int(ni.value)
+
     def adjoint(self, dpos, dnrm, count: int, dfield):
         _check(lib().HPMCextractVerticesAdjoint(self.ptr, _ptr(dpos), _ptr(dnrm), int(count),
                                                 dfield.data_ptr()), "HPMCextractVerticesAdjoint")

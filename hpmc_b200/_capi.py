@@ -84,6 +84,8 @@ _SIGS = {
     "HPMCgetClassifyPath": (C.c_int, [vp, C.POINTER(C.c_int)]),
     "HPMCextractStatic": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_float,
                                     C.c_int, C.POINTER(C.c_float), vp, vp, C.c_size_t, vp, vp]),
+    "HPMCextractVerticesIndexed": (C.c_int, [vp, vp, vp, C.c_size_t, vp, C.c_size_t, C.POINTER(C.c_uint64),
+                                             C.POINTER(C.c_uint64)]),
     # batched extraction
     "HPMCcreateBatch": (C.c_int, [vp, vp, C.c_int, C.POINTER(vp)]),
     "HPMCdestroyBatch": (None, [vp]),

@@ -97,6 +97,9 @@ struct HPMCTraversalHandle {
     size_t feedback_cap = 0;
     int32_t* dbg_cell = nullptr;
     float* dbg_t = nullptr;
+    // indexed-mesh scratch (grown on demand, one allocation)
+    unsigned char* mesh_mem = nullptr;
+    size_t mesh_cap = 0;  // soup vertices it was sized for
 };
 
 namespace {
@@ -505,6 +508,10 @@ HPMCTraversalHandle* HPMCcreateTraversalHandle(HPMCHistoPyramid* h) {
 
 void HPMCdestroyTraversalHandle(HPMCTraversalHandle* th) {
     if (!th || th->magic != kMagicTraversal) return;
+    if (th->mesh_mem) {
+        cudaDeviceSynchronize();
+        cudaFree(th->mesh_mem);
+    }
     th->magic = 0;
     delete th;
 }
@@ -671,6 +678,72 @@ int HPMCextractVerticesAdjoint(HPMCTraversalHandle* th, const float* dpos, const
         return HPMC_ERR_CUDA;
     }
     return HPMC_OK;
+}
+
+int HPMCextractVerticesIndexed(HPMCTraversalHandle* th, float* positions, float* normals, size_t vertex_capacity,
+                               uint32_t* indices, size_t index_capacity, uint64_t* n_vertices, uint64_t* n_indices) {
+    if (!valid(th)) return HPMC_ERR_INVALID_HANDLE;
+    HPMCHistoPyramid* h = th->h;
+    if (h->broken) return HPMC_ERR_BROKEN;
+    if (!h->built) return HPMC_ERR_NOT_BUILT;
+    if ((positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16) ||
+        (indices && (uintptr_t)indices % 4))
+        return HPMC_ERR_INVALID_VALUE;
+    const GLuint n = HPMCacquireNumberOfVertices(h);  // sizes the scratch (host sync)
+    if (n == 0 && h->status != HPMC_OK) return h->status;
+    // scratch: keys | table keys | first | scan | table vals | tile sums | meta | unique count
+    size_t tsize = 1;
+    while (tsize < 2 * (size_t)n + 2) tsize <<= 1;
+    const size_t tiles = (size_t)n / 2048 + 2;
+    auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+    const size_t o_keys = 0, o_tkeys = up(o_keys + 8 * (size_t)n), o_first = up(o_tkeys + 8 * tsize),
+                 o_scan = up(o_first + 4 * (size_t)n), o_tvals = up(o_scan + 4 * (size_t)n),
+                 o_tiles = up(o_tvals + 4 * tsize), o_meta = up(o_tiles + 4 * tiles),
+                 o_unique = up(o_meta + 2 * (size_t)n), bytes = o_unique + 256;
+    if (!th->mesh_mem || th->mesh_cap < bytes) {
+        if (th->mesh_mem) {
+            cudaStreamSynchronize(h->stream);
+            cudaFree(th->mesh_mem);
+        }
+        th->mesh_mem = nullptr;
+        th->mesh_cap = 0;
+        if (cudaMalloc(&th->mesh_mem, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return HPMC_ERR_OUT_OF_MEMORY;
+        }
+        th->mesh_cap = bytes;
+    }
+    unsigned char* m = th->mesh_mem;
+    hpmc::MeshIO M{};
+    M.count = n;
+    M.keys = reinterpret_cast<unsigned long long*>(m + o_keys);
+    M.table_keys = reinterpret_cast<unsigned long long*>(m + o_tkeys);
+    M.first = reinterpret_cast<uint32_t*>(m + o_first);
+    M.scan = reinterpret_cast<uint32_t*>(m + o_scan);
+    M.table_vals = reinterpret_cast<uint32_t*>(m + o_tvals);
+    M.tile_sums = reinterpret_cast<uint32_t*>(m + o_tiles);
+    M.meta = reinterpret_cast<uint16_t*>(m + o_meta);
+    M.unique = reinterpret_cast<unsigned long long*>(m + o_unique);
+    M.table_mask = (uint32_t)(tsize - 1);
+    M.pos = reinterpret_cast<float4*>(positions);
+    M.nrm = reinterpret_cast<float4*>(normals);
+    M.vcap = vertex_capacity;
+    M.indices = indices;
+    M.icap = index_capacity;
+    const int grid = h->constants->num_sms * 8;
+    cudaError_t e = hpmc::launch_mesh(h->V, M, h->normal_mode, traverse_grid(h), grid, h->stream);
+    unsigned long long unique = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&unique, M.unique, sizeof unique, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(h, HPMC_ERR_CUDA, true);
+        return HPMC_ERR_CUDA;
+    }
+    if (n == 0) unique = 0;
+    if (n_vertices) *n_vertices = unique;
+    if (n_indices) *n_indices = n;
+    return (unique > vertex_capacity || (size_t)n > index_capacity) ? HPMC_ERR_CAPACITY : HPMC_OK;
 }
 
 int HPMCsetCodeCapture(HPMCHistoPyramid* h, uint8_t* device_codes) {

@@ -50,6 +50,27 @@ struct BatchDev {
     int rounds;                    // traversal rounds of 32 vertices per work item
 };
 
+// Indexed-mesh extraction: scratch and outputs (device).
+struct MeshIO {
+    uint32_t count;                  // soup vertices (the vertex count of the build)
+    unsigned long long* keys;        // count: edge key per soup vertex
+    uint16_t* meta;                  // count: case | vertex-in-cell << 8
+    unsigned long long* table_keys;  // table_mask + 1 (>= 2 count, power of two)
+    uint32_t* table_vals;
+    uint32_t table_mask;
+    uint32_t* first;                 // count
+    uint32_t* scan;                  // count
+    uint32_t* tile_sums;             // count / 2048 + 1
+    unsigned long long* unique;      // 1: unique vertices
+    float4* pos;                     // unique vertices (may be null)
+    float4* nrm;
+    unsigned long long vcap;
+    uint32_t* indices;               // one per soup vertex (may be null)
+    unsigned long long icap;
+};
+
+cudaError_t launch_mesh(const Volume& V, const MeshIO& M, int normal_mode, int traverse_grid, int grid,
+                        cudaStream_t st);
 cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ctas, cudaStream_t st);
 cudaError_t launch_classify_batch(const BatchDev& B, int ftype, unsigned int bricks, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchDev& B, unsigned int chunks, cudaStream_t st);

@@ -549,6 +549,240 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_batch(const __grid_const
 }
 
 // ---------------------------------------------------------------------------
+// Indexed (welded) output.  No counterpart in the reference, which emits
+// triangle soup only.  Every soup vertex lies on a lattice edge (a, axis);
+// welding keeps one vertex per edge, numbered in order of first occurrence
+// in the soup, and an index per soup vertex (three per triangle, the soup's
+// triangle order).
+//   mesh_keys   traversal without geometry: the edge key of every soup vertex
+//               (and its case / vertex-in-cell, for binary-field normals);
+//   mesh_insert open-addressing table key -> smallest soup index (atomicCAS
+//               on the key, atomicMin on the index);
+//   mesh_first  per soup vertex: that smallest index, and a flag "first";
+//   mesh_scan_* exclusive scan of the flags = unique vertex numbers;
+//   mesh_emit   indices, and the geometry of each unique vertex computed once
+//               from its edge (bit-identical to the soup vertex's).
+__device__ __forceinline__ unsigned long long edge_key(const Volume& V, const int a[3], int axis) {
+    return ((((unsigned long long)a[2] * (unsigned long long)V.lattice[1]) + (unsigned long long)a[1]) *
+                (unsigned long long)V.lattice[0] + (unsigned long long)a[0]) * 3ull + (unsigned long long)axis;
+}
+
+__global__ void __launch_bounds__(kThreads, 4) mesh_keys(const __grid_constant__ Volume V, unsigned long long* keys,
+                                                         uint16_t* meta, uint32_t count) {
+    extern __shared__ __align__(16) uint8_t s_traverse[];
+    TraverseSmem& S = *reinterpret_cast<TraverseSmem*>(s_traverse);
+    load_tables(V, S);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long total = V.ctrl->total;
+    const uint32_t N = (uint32_t)(total < count ? total : count);
+    const uint32_t rounds = item_rounds(N, gridDim.x);
+    const uint32_t VW = 32u * rounds;
+    const uint32_t nchunks = (N + VW - 1) / VW;
+    WarpBlock B;
+    B.have = false;
+    for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
+#pragma unroll 1
+        for (uint32_t r = 0; r < rounds; r++) {
+            const uint32_t v = chunk * VW + 32u * r + lane;
+            const bool act = v < N;
+            if (!__any_sync(0xffffffffu, act)) break;
+            VertexCell c;
+            if (!resolve_vertex(V, S, warp, lane, v, act, B, c)) continue;
+            const EdgeGeom g = edge_of(S, c);
+            keys[v] = edge_key(V, g.a, g.axis);
+            meta[v] = (uint16_t)(c.code | (c.k << 8));
+        }
+    }
+    finish_queue(V);
+}
+
+constexpr unsigned long long kEmptyKey = ~0ull;
+
+__device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    return (uint32_t)k;
+}
+
+__global__ void mesh_insert(const unsigned long long* keys, uint32_t n, unsigned long long* tkeys, uint32_t* tvals,
+                            uint32_t mask, unsigned int* status) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[i];
+        uint32_t h = key_hash(key) & mask;
+        bool done = false;
+        for (uint32_t probe = 0; probe <= mask; probe++) {  // the table has >= 2n slots: ends long before
+            const unsigned long long prev = atomicCAS(&tkeys[h], kEmptyKey, key);
+            if (prev == kEmptyKey || prev == key) {
+                atomicMin(&tvals[h], i);
+                done = true;
+                break;
+            }
+            h = (h + 1u) & mask;
+        }
+        if (!done) atomicOr(status, kStatusCapacity);
+    }
+}
+
+__device__ __forceinline__ uint32_t table_find(const unsigned long long* tkeys, const uint32_t* tvals, uint32_t mask,
+                                               unsigned long long key) {
+    uint32_t h = key_hash(key) & mask;
+    for (uint32_t probe = 0; probe <= mask; probe++) {
+        const unsigned long long k = tkeys[h];
+        if (k == key) return tvals[h];
+        if (k == kEmptyKey) break;
+        h = (h + 1u) & mask;
+    }
+    return 0xffffffffu;
+}
+
+constexpr int kScanItems = 8;                        // per thread
+constexpr uint32_t kScanTile = kThreads * kScanItems; // per CTA
+
+__global__ void __launch_bounds__(kThreads) mesh_first(const unsigned long long* keys, uint32_t n,
+                                                       const unsigned long long* tkeys, const uint32_t* tvals,
+                                                       uint32_t mask, uint32_t* first, uint32_t* scan,
+                                                       uint32_t* tile_sums) {
+    // first[i] = smallest soup index of i's edge; scan[i] = exclusive count of
+    // firsts within the tile; tile_sums[tile] = firsts in the tile
+    __shared__ uint32_t s_warp[kWarps];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t f[kScanItems], sum = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const uint32_t i = base + j;
+        uint32_t fi = 0u;
+        if (i < n) {
+            const uint32_t m = table_find(tkeys, tvals, mask, keys[i]);
+            first[i] = m;
+            fi = (m == i) ? 1u : 0u;
+        }
+        f[j] = fi;
+        sum += fi;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    uint32_t off = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; w++) {
+        if (w < warp) off += s_warp[w];
+        tot += s_warp[w];
+    }
+    uint32_t run = off + inc - sum;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const uint32_t i = base + j;
+        if (i < n) scan[i] = run;
+        run += f[j];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// One CTA: exclusive scan of the tile sums in place; total into *unique.
+__global__ void __launch_bounds__(kThreads) mesh_scan_tiles(uint32_t* tile_sums, uint32_t ntiles,
+                                                            unsigned long long* unique) {
+    __shared__ uint32_t s_warp[kWarps];
+    uint32_t carry = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t b = 0; b < ntiles; b += kThreads) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t x = i < ntiles ? tile_sums[i] : 0u;
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        uint32_t off = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; w++) {
+            if (w < warp) off += s_warp[w];
+            tot += s_warp[w];
+        }
+        if (i < ntiles) tile_sums[i] = carry + off + inc - x;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *unique = carry;
+}
+
+template <int FT, int MODE>
+__global__ void __launch_bounds__(kThreads) mesh_emit(const __grid_constant__ Volume V, const unsigned long long* keys,
+                                                      const uint16_t* meta, uint32_t n, const uint32_t* first,
+                                                      const uint32_t* scan, const uint32_t* tile_sums, float4* pos,
+                                                      float4* nrm, unsigned long long vcap, uint32_t* indices,
+                                                      unsigned long long icap) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = first[i];
+        if (j >= n) continue;  // not found: the insert reported it
+        const uint32_t u = scan[j] + tile_sums[j / kScanTile];
+        if (indices && i < icap) indices[i] = u;
+        if (j != i || u >= vcap) continue;
+        // the unique vertex: geometry from its edge
+        const unsigned long long key = keys[i];
+        const int axis = (int)(key % 3ull);
+        unsigned long long r = key / 3ull;
+        int a[3];
+        a[0] = (int)(r % (unsigned long long)V.lattice[0]);
+        r /= (unsigned long long)V.lattice[0];
+        a[1] = (int)(r % (unsigned long long)V.lattice[1]);
+        a[2] = (int)(r / (unsigned long long)V.lattice[1]);
+        const uint16_t m = meta[i];
+        const int code = m & 0xff, k = (m >> 8) & 15;
+        float p[3], nn[3], t;
+        edge_vertex<FT, MODE>(V, a, axis, a[0], a[1], a[2], g_binary_normals + 3 * (16 * code + k), p, nn, t);
+        if (pos) pos[u] = make_float4(p[0], p[1], p[2], 1.0f);
+        if (nrm) nrm[u] = make_float4(nn[0], nn[1], nn[2], 0.0f);
+    }
+}
+
+cudaError_t launch_mesh(const Volume& V, const MeshIO& M, int normal_mode, int traverse_grid, int grid,
+                        cudaStream_t st) {
+    const uint32_t n = M.count;
+    mesh_keys<<<traverse_grid, kThreads, kTraverseSmem, st>>>(V, M.keys, M.meta, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || n == 0) return e;
+    if ((e = cudaMemsetAsync(M.table_keys, 0xff, sizeof(unsigned long long) * (M.table_mask + 1ull), st)) !=
+            cudaSuccess ||
+        (e = cudaMemsetAsync(M.table_vals, 0xff, sizeof(uint32_t) * (M.table_mask + 1ull), st)) != cudaSuccess)
+        return e;
+    mesh_insert<<<grid, kThreads, 0, st>>>(M.keys, n, M.table_keys, M.table_vals, M.table_mask, &V.ctrl->status);
+    const uint32_t ntiles = (n + kScanTile - 1) / kScanTile;
+    mesh_first<<<ntiles, kThreads, 0, st>>>(M.keys, n, M.table_keys, M.table_vals, M.table_mask, M.first, M.scan,
+                                            M.tile_sums);
+    mesh_scan_tiles<<<1, kThreads, 0, st>>>(M.tile_sums, ntiles, M.unique);
+    const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
+#define HPMC_MESH_EMIT(FT_, MODE_)                                                                             \
+    mesh_emit<FT_, MODE_><<<grid, kThreads, 0, st>>>(V, M.keys, M.meta, n, M.first, M.scan, M.tile_sums, M.pos,  \
+                                                     M.nrm, M.vcap, M.indices, M.icap)
+#define HPMC_MESH_CASE(FT_)                                                                                    \
+    case FT_:                                                                                                  \
+        if (mode == kModeBinary) HPMC_MESH_EMIT(FT_, kModeBinary);                                             \
+        else if (mode == kModeCentral) HPMC_MESH_EMIT(FT_, kModeCentral);                                      \
+        else HPMC_MESH_EMIT(FT_, kModeForward);                                                                \
+        break;
+    switch (V.ftype) {
+        HPMC_MESH_CASE(kFieldF32)
+        HPMC_MESH_CASE(kFieldU8)
+        HPMC_MESH_CASE(kFieldUNorm8)
+        HPMC_MESH_CASE(kFieldFunctor)
+        default: return cudaErrorInvalidValue;
+    }
+#undef HPMC_MESH_CASE
+#undef HPMC_MESH_EMIT
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st) {
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);

@@ -245,6 +245,22 @@ int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
  * per-block kernel (narrow tiles, unaligned pitches, functor fields). */
 int HPMCgetClassifyPath(struct HPMCHistoPyramid* h, int* path);
 
+/* ---- indexed (welded) output ----
+ *
+ * No counterpart in the reference, which emits triangle soup only.  One
+ * vertex per crossed lattice edge, numbered in order of first occurrence in
+ * the soup of HPMCextractVertices, written as float4 positions / normals
+ * (either may be NULL), and one uint32 index per soup vertex -- three per
+ * triangle, in the soup's triangle order.  A unique vertex's values equal
+ * those of its soup vertices (binary fields: the normal of its first
+ * occurrence, as table normals depend on the cell's case).  Waits for the
+ * result; n_vertices / n_indices receive the full counts (HPMC_ERR_CAPACITY
+ * if an output was too small: what fits is written).  Device scratch of
+ * about 40 bytes per soup vertex is kept with the traversal handle. */
+int HPMCextractVerticesIndexed(struct HPMCTraversalHandle* th, float* positions, float* normals,
+                               size_t vertex_capacity, uint32_t* indices, size_t index_capacity,
+                               uint64_t* n_vertices, uint64_t* n_indices);
+
 /* ---- batched extraction ----
  *
  * No counterpart in the reference, which builds one volume per HistoPyramid
