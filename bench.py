@@ -7,10 +7,13 @@ position/normal streams (HPMCextractVertices, vertex count read on the device).
 
   value    Gcells/s with the field resident in HBM (device time, CUDA events)
   e2e      the same through the public API with host buffers: pinned H2D of
-           the field, build, count (host sync), extraction, D2H of every vertex
+           the field, build, count (host sync), extraction, D2H of every vertex;
+           two volumes in flight (two handles on two streams: the H2D of
+           volume k+1 overlaps volume k); the one-at-a-time figure beside it
   roofline the build kernels (classify + reduce) against measured HBM copy
            bandwidth; algorithmic bytes = field bytes read once
-  cpu_baseline  the oracle (CPU restatement of the reference) on a z-slab sample
+  cpu_baseline  the reference's generated shader passes run as C++ on the host
+           cores (the oracle restatement if they cannot be built), z-slab sample
   batched  64 uneven FP32 volumes: batched extractor (CUDA-graph replay) vs
            the plain per-volume loop through the handle API, volumes/s
   adjoint  128^3 sphere SDF: adjoint (backward) time over forward time
@@ -414,25 +417,34 @@ def run_hpmc(args, rank, world, local_rank):
     stream.synchronize()
 
     # --- timed region: field resident in HBM -------------------------------
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+    # K steps back to back with events only at the ends: an event recorded
+    # between two launches costs several microseconds and cuts the launches'
+    # programmatic overlap (~12 us per step measured at 512^3).
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    if True:
-        t_begin = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_begin.record(stream)
-        for i in range(args.steps):
-            ev[3 * i].record(stream)
-            hp.build(iso)
-            ev[3 * i + 1].record(stream)
-            th.extract()
-            ev[3 * i + 2].record(stream)
-        t_end.record(stream)
-        stream.synchronize()
-        torch.cuda.synchronize()
-    clocks.stop()
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_begin.record(stream)
+    for _ in range(args.steps):
+        step()
+    t_end.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
     total_ms = t_begin.elapsed_time(t_end)
+
+    # --- kernel breakdown: a second pass of K steps with events around the
+    # build (classify + reduce) and the extraction of every step
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * args.steps)]
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        ev[3 * i].record(stream)
+        hp.build(iso)
+        ev[3 * i + 1].record(stream)
+        th.extract()
+        ev[3 * i + 2].record(stream)
+    stream.synchronize()
+    clocks.stop()
     build_ms = [ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps)]
     trav_ms = [ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps)]
     total_ms = multi.max_over_ranks(total_ms, device=dev)
@@ -450,41 +462,96 @@ def run_hpmc(args, rank, world, local_rank):
             "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes,
             "traffic_source": "ncu dram__bytes_read+write of the 384^3 capture, scaled by field bytes",
             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": field_bytes,
-            "avg_launch_ms": build_avg}
+            "avg_launch_ms": build_avg,
+            "timing": "CUDA events around every build of a second pass of K steps on the launching stream"}
     step_frac = alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak
 
     # --- e2e through the public API with host buffers ----------------------
+    # Every step copies its field from pinned host memory, builds, reads the
+    # count on the host, extracts and copies every vertex back.  Serial: one
+    # volume at a time.  Pipelined (the reported value): two handles on two
+    # streams, so the H2D copy of volume k+1 runs while volume k is built,
+    # extracted and copied back (PCIe is full duplex).
     e2e = None
     if not args.no_e2e:
         h_field = torch.from_numpy(field_np).pin_memory()
-        h_pos = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
-        h_nrm = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
-        e2e_steps = max(3, min(args.steps, 10))
-        with torch.cuda.stream(stream):
-            for _ in range(2):
-                field.copy_(h_field, non_blocking=True)
-                hp.build(iso)
-                n = hp.acquire_number_of_vertices()
-                th.extract()
-                h_pos[:n].copy_(pos[:n], non_blocking=True)
-                h_nrm[:n].copy_(nrm[:n], non_blocking=True)
-            stream.synchronize()
+        e2e_steps = max(4, min(args.steps, 10))
+
+        class Slot:
+            pass
+
+        slots = []
+        for k in range(2):
+            sl = Slot()
+            sl.h_pos = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
+            sl.h_nrm = torch.empty((nverts, 4), dtype=torch.float32).pin_memory()
+            if k == 0:
+                sl.stream, sl.hp, sl.th, sl.field, sl.pos, sl.nrm = stream, hp, th, field, pos, nrm
+            else:
+                sl.stream = torch.cuda.Stream(device=dev)
+                sl.field = torch.empty_like(field)
+                sl.hp = H.HistoPyramid(C)
+                sl.hp.set_stream(sl.stream)
+                sl.hp.set_field_device(sl.field)
+                sl.hp.set_normal_mode(H.NORMALS_CENTRAL)
+                sl.th = H.TraversalHandle(sl.hp)
+                sl.pos = torch.empty_like(pos)
+                sl.nrm = torch.empty_like(nrm)
+                sl.th.set_buffers(sl.pos, sl.nrm, nverts)
+            slots.append(sl)
+        counts = []
+
+        def issue_in(k):  # H2D + build of volume k
+            sl = slots[k % 2]
+            with torch.cuda.stream(sl.stream):
+                sl.field.copy_(h_field, non_blocking=True)
+            sl.hp.build(iso)
+
+        def finish(k):  # count (host sync), extraction, D2H of volume k
+            sl = slots[k % 2]
+            n = sl.hp.acquire_number_of_vertices()
+            counts.append(n)
+            sl.th.extract()
+            with torch.cuda.stream(sl.stream):
+                sl.h_pos[:n].copy_(sl.pos[:n], non_blocking=True)
+                sl.h_nrm[:n].copy_(sl.nrm[:n], non_blocking=True)
+
+        def serial(steps):
+            for k in range(steps):
+                issue_in(0)
+                finish(0)
+
+        def pipelined(steps):
+            issue_in(0)
+            for k in range(steps):
+                if k + 1 < steps:
+                    issue_in(k + 1)
+                finish(k)
+
+        def timed(fn, steps):
+            torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(e2e_steps):
-                field.copy_(h_field, non_blocking=True)
-                hp.build(iso)
-                n = hp.acquire_number_of_vertices()
-                th.extract()
-                h_pos[:n].copy_(pos[:n], non_blocking=True)
-                h_nrm[:n].copy_(nrm[:n], non_blocking=True)
+            slots[1].stream.wait_event(e0)
+            fn(steps)
+            stream.wait_stream(slots[1].stream)
             e1.record(stream)
-            stream.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / e2e_steps
-        assert n == nverts
-        e2e = {"value": cells / (e2e_ms * 1e-3) / 1e9, "unit": "Gcells/s", "h2d_bytes_per_step": field_bytes,
-               "d2h_bytes_per_step": 32 * nverts, "ms_per_step": e2e_ms}
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / steps
+
+        serial(2)  # warm-up of both legs
+        pipelined(3)
+        serial_ms = timed(serial, e2e_steps)
+        e2e_ms = timed(pipelined, e2e_steps)
+        assert all(n == nverts for n in counts), counts
+        assert torch.equal(slots[0].h_pos[:nverts], slots[1].h_pos[:nverts])
+        serial_ms = multi.max_over_ranks(serial_ms, device=dev)
+        e2e_ms = multi.max_over_ranks(e2e_ms, device=dev)
+        e2e = {"value": cells * world / (e2e_ms * 1e-3) / 1e9, "unit": "Gcells/s", "h2d_bytes_per_step": field_bytes,
+               "d2h_bytes_per_step": 32 * nverts, "ms_per_step": e2e_ms, "volumes_in_flight": 2,
+               "serial_value": cells * world / (serial_ms * 1e-3) / 1e9, "serial_ms_per_step": serial_ms}
+        del slots
 
     batched = None
     if not args.no_batch:

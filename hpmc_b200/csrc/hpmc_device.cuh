@@ -194,4 +194,34 @@ __host__ __device__ __forceinline__ uint64_t column_block_index(const Volume& V,
     return (uint64_t)(morton_spread16(X0 >> 5) | (morton_spread16(Y0 >> 5) << 1));
 }
 
+// Programmatic dependent launch.  The step's kernels (classify, reduce,
+// traverse) are launched with programmatic stream serialization, so a
+// kernel's CTAs may become resident while the previous kernel on the stream
+// is still running.  Every thread calls wait_prior_grid() before it reads or
+// writes global memory that earlier stream work may touch; it returns once
+// the previous grid has completed and its writes are visible (at once when
+// the launch had no such attribute).  allow_next_grid() lets the next kernel
+// launch its CTAs early; they wait in their own wait_prior_grid().
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+#ifdef __CUDACC__
+// Host: launch `kernel` on `st` with programmatic stream serialization.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                    const Args&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#endif
+
 }  // namespace hpmc

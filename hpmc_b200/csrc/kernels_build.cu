@@ -382,6 +382,10 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
         mbar_fence_init();
     }
+    // global memory (field, pyramid, control block) only after the previous
+    // grid.  No early trigger: the reduce launches as these CTAs exit (reduce
+    // CTAs resident and waiting through the whole build measured ~2% slower).
+    wait_prior_grid();
     __syncthreads();
     // producer state (thread 0): next box to issue = box pk of column pu
     int pu = blockIdx.x, pk = 0;
@@ -586,11 +590,15 @@ __global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant_
     __shared__ __align__(16) uint32_t buf0[kReduceTop];
     __shared__ uint32_t buf1[kReduceTop / 4];
     __shared__ int s_last;
+    wait_prior_grid();
+    allow_next_grid();
     reduce_chunk(V, j_in, j_stop, mask_level5, blockIdx.x, gridDim.x, buf0, buf1, &s_last);
 }
 
 // Top entry when the whole pyramid is one block (no reduction launch needed).
 __global__ void copy_total(const __grid_constant__ Volume V) {
+    wait_prior_grid();
+    allow_next_grid();
     if (threadIdx.x == 0) V.ctrl->total = V.levels[V.level_off[V.jtop]];
 }
 
@@ -736,11 +744,12 @@ cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ct
         const int slots = (max_ctas / 16) * column_ctas_per_sm();
         const int grid = ncolumns < slots ? ncolumns : slots;
         if (V.ftype == kFieldF32)
-            classify_columns<kFieldF32><<<grid, kThreads, kRingBytesF32, st>>>(*tmap, V, ncolumns);
+            return launch_dependent(classify_columns<kFieldF32>, grid, kThreads, kRingBytesF32, st, *tmap, V, ncolumns);
         else if (V.ftype == kFieldU8)
-            classify_columns<kFieldU8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V, ncolumns);
+            return launch_dependent(classify_columns<kFieldU8>, grid, kThreads, kRingBytesU8, st, *tmap, V, ncolumns);
         else
-            classify_columns<kFieldUNorm8><<<grid, kThreads, kRingBytesU8, st>>>(*tmap, V, ncolumns);
+            return launch_dependent(classify_columns<kFieldUNorm8>, grid, kThreads, kRingBytesU8, st, *tmap, V,
+                                    ncolumns);
     } else {
         const long long nb = V.nblocks;
         const int grid = (int)(nb < (long long)max_ctas ? nb : (long long)max_ctas);
@@ -755,19 +764,15 @@ cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ct
 }
 
 cudaError_t launch_reduce(const Volume& V, cudaStream_t st) {
-    if (V.jtop == kBlockLevel) {
-        copy_total<<<1, 32, 0, st>>>(V);
-        return cudaGetLastError();
-    }
+    if (V.jtop == kBlockLevel) return launch_dependent(copy_total, 1, 32, 0, st, V);
     int j_in = kBlockLevel;
     while (j_in < V.jtop) {
         // one launch reduces 5 levels per CTA plus up to 6 more in the last CTA
         const int j_stop = (V.jtop - j_in <= 11) ? V.jtop : j_in + 5;
         const long long n_in = level_entries(V.size_l2, j_in);
         const long long grid = (n_in + kReduceChunk - 1) / kReduceChunk;
-        reduce_levels<<<(unsigned)grid, kThreads, 0, st>>>(V, j_in, j_stop,
-                                                            (j_in == kBlockLevel && V.column_layout) ? 1 : 0);
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e = launch_dependent(reduce_levels, (unsigned)grid, kThreads, 0, st, V, j_in, j_stop,
+                                         (j_in == kBlockLevel && V.column_layout) ? 1 : 0);
         if (e != cudaSuccess) return e;
         j_in = j_stop;
     }

@@ -95,6 +95,9 @@ __device__ __forceinline__ void load_base_tables(TraverseSmem& S) {
 
 __device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
     load_base_tables(S);
+    // the pyramid and the control block only after the previous grid (the
+    // build).  No early trigger: the next build launches as these CTAs exit.
+    wait_prior_grid();
     for (int i = threadIdx.x; i < V.top_cached; i += blockDim.x) S.top[i] = V.levels[i];
     __syncthreads();
 }
@@ -786,12 +789,13 @@ cudaError_t launch_mesh(const Volume& V, const MeshIO& M, int normal_mode, int t
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st) {
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
-#define HPMC_TRAVERSE_CASE(FT_)                                                                        \
-    case FT_:                                                                                          \
-        if (mode == kModeBinary) traverse_kernel<FT_, kModeBinary><<<grid, kThreads, kTraverseSmem, st>>>(V, O);   \
-        else if (mode == kModeCentral) traverse_kernel<FT_, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, O); \
-        else traverse_kernel<FT_, kModeForward><<<grid, kThreads, kTraverseSmem, st>>>(V, O);                     \
-        break;
+#define HPMC_TRAVERSE_CASE(FT_)                                                                              \
+    case FT_:                                                                                                \
+        if (mode == kModeBinary)                                                                             \
+            return launch_dependent(traverse_kernel<FT_, kModeBinary>, grid, kThreads, kTraverseSmem, st, V, O);  \
+        if (mode == kModeCentral)                                                                            \
+            return launch_dependent(traverse_kernel<FT_, kModeCentral>, grid, kThreads, kTraverseSmem, st, V, O); \
+        return launch_dependent(traverse_kernel<FT_, kModeForward>, grid, kThreads, kTraverseSmem, st, V, O);
     switch (V.ftype) {
         HPMC_TRAVERSE_CASE(kFieldF32)
         HPMC_TRAVERSE_CASE(kFieldU8)
@@ -800,7 +804,6 @@ cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mo
         default: return cudaErrorInvalidValue;
     }
 #undef HPMC_TRAVERSE_CASE
-    return cudaGetLastError();
 }
 
 cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode, int grid, cudaStream_t st) {
