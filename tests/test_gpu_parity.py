@@ -130,6 +130,27 @@ def test_config_noise_u8_256_ties(hpmc, oracle):
     assert rep["n"] > 2**24
 
 
+@pytest.mark.slow
+def test_config_cayley_512_full_size(hpmc, oracle):
+    """The benchmark workload at its full size (FP32 512^3 Cayley cubic, iso 0,
+    central normals, the TMA column path): every case index, every dense
+    level, the count, the vertex order and the geometry of all vertices; a
+    second build + extraction is bit-identical (the persistent traversal's
+    dynamic work assignment does not change the output)."""
+    from hpmc_b200 import datasets
+
+    field, iso = datasets.cayley(512)
+    g = run_gpu(hpmc, field, iso, normals=1)
+    assert g["path"] == 1  # the TMA column classifier
+    e = oracle_expect(oracle, field, iso, normals=1)
+    rep = compare(g, e)
+    assert rep["n"] > 3_000_000
+    g2 = run_gpu(hpmc, field, iso, normals=1, capture_codes=False)
+    assert g2["n"] == g["n"]
+    assert np.array_equal(g2["pos"].view(np.uint32), g["pos"].view(np.uint32))
+    assert np.array_equal(g2["nrm"].view(np.uint32), g["nrm"].view(np.uint32))
+
+
 def test_binary_mode_and_feedback_capture(hpmc, oracle):
     """Binary fields (midpoints + table normals) and the N3F_V3F capture."""
     import torch
