@@ -151,6 +151,52 @@ def test_config_cayley_512_full_size(hpmc, oracle):
     assert np.array_equal(g2["nrm"].view(np.uint32), g["nrm"].view(np.uint32))
 
 
+def test_caller_kernels_on_the_stream_stay_ordered(hpmc, oracle):
+    """The build and extraction launch with programmatic stream serialization.
+    A caller's kernel that rewrites the field right before a build, or the
+    output right after an extraction, on the same stream must still be fully
+    ordered with them: alternate two fields through one device buffer."""
+    import torch
+
+    from hpmc_b200 import datasets
+
+    dev = torch.device("cuda:0")
+    fa, iso = datasets.cayley(96)
+    fb = np.ascontiguousarray(fa[:, :, ::-1] * np.float32(1.5) + np.float32(0.01))
+    ea = oracle_expect(oracle, fa, iso, normals=1)
+    eb = oracle_expect(oracle, fb, iso, normals=1)
+    assert ea["total"] != eb["total"]
+    src = [torch.from_numpy(fa).to(dev), torch.from_numpy(fb).to(dev)]
+    exp = [ea, eb]
+    buf = torch.empty_like(src[0])
+    stream = torch.cuda.Stream(device=dev)
+    hp = hpmc.HistoPyramid(hpmc.default_constants())
+    hp.set_stream(stream)
+    hp.set_field_device(buf)
+    hp.set_normal_mode(1)
+    th = hpmc.TraversalHandle(hp)
+    cap = max(ea["total"], eb["total"])
+    pos = torch.empty((cap, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((cap, 4), dtype=torch.float32, device=dev)
+    th.set_buffers(pos, nrm, cap)
+    for i in range(6):
+        e = exp[i % 2]
+        with torch.cuda.stream(stream):
+            torch.mul(src[i % 2], 1.0, out=buf)  # a kernel, not a copy
+        hp.build(iso)
+        n = hp.acquire_number_of_vertices()
+        assert n == e["total"], (i, n, e["total"])
+        th.extract()
+        with torch.cuda.stream(stream):
+            snap = pos[:n].clone()  # a kernel reading the output right after the extraction
+            pos.fill_(float("nan"))
+        stream.synchronize()
+        dp = np.abs(snap[:, :3].cpu().numpy().astype(np.float64) - e["pos"])
+        assert dp.max() <= 1e-5 / 95 + 1e-6, (i, dp.max())
+    th.close()
+    hp.close()
+
+
 def test_binary_mode_and_feedback_capture(hpmc, oracle):
     """Binary fields (midpoints + table normals) and the N3F_V3F capture."""
     import torch
