@@ -54,6 +54,9 @@ FALLBACK_HBM_GBS = 6650.0
 BUILD_TRAFFIC_PER_FIELD_BYTE = (226560000 + 8833024 + 1067264) / 226492416
 
 
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e nominal (DGX figure), reported beside the measured copy peak
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:
@@ -463,7 +466,8 @@ def run_hpmc(args, rank, world, local_rank):
             "traffic_source": "ncu dram__bytes_read+write of the 384^3 capture, scaled by field bytes",
             "peak_kind": peak_kind, "algorithmic_bytes_per_launch": field_bytes,
             "avg_launch_ms": build_avg,
-            "timing": "CUDA events around every build of a second pass of K steps on the launching stream"}
+            "timing": "CUDA events around every build of a second pass of K steps on the launching stream",
+            "frac_of_nominal": field_bytes / (build_avg * 1e-3) / 1e9 / NOMINAL_HBM_GBS}
     step_frac = alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak
 
     # --- e2e through the public API with host buffers ----------------------
@@ -576,6 +580,7 @@ def run_hpmc(args, rank, world, local_rank):
                            "parallelism": f"replicas x{world} (independent volumes)"},
                 "roofline": roof,
                 "step_hbm_fraction": step_frac,
+                "step_hbm_fraction_of_nominal": alg_bytes / (ms_per_step * 1e-3) / 1e9 / NOMINAL_HBM_GBS,
                 "step_algorithmic_bytes": alg_bytes,
                 "vertices_per_s": nverts * world * args.steps / (total_ms * 1e-3),
                 "build_ms": build_avg, "traverse_ms": trav_avg,

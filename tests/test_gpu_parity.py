@@ -151,6 +151,52 @@ def test_config_cayley_512_full_size(hpmc, oracle):
     assert np.array_equal(g2["nrm"].view(np.uint32), g["nrm"].view(np.uint32))
 
 
+def test_product_layout_matches_oracle(hpmc, oracle):
+    """The product's own HPMCdetermineLayout (init.cpp:72-149) against the
+    oracle's, which is pinned to the reference's compiled init.cpp: the
+    survey's sizes, 300 random lattices and grids, and the sizes the
+    reference rejects (an axis below 2 or above 16384 samples, a grid not
+    smaller than the lattice), which fail lazily with HPMC_ERR_LAYOUT."""
+    import torch
+
+    from hpmc_b200 import _capi
+
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(23)
+    cases = [((32, 32, 32), None), ((36, 36, 36), None), ((64, 64, 64), None), ((128, 128, 128), None),
+             ((192, 192, 192), None), ((301, 301, 301), None), ((301, 324, 56), None), ((2, 2, 2), None),
+             ((16384, 2, 2), None), ((2, 16384, 2), None), ((2, 2, 16384), None), ((3, 3, 3), None),
+             ((16385, 2, 2), None), ((2, 2, 16385), None), ((1, 5, 5), None), ((8, 8, 8), (8, 7, 7)),
+             ((8, 8, 8), (7, 9, 7))]
+    while len(cases) < 317:
+        lat = tuple(int(v) for v in np.exp(rng.uniform(np.log(2), np.log(400), 3)).astype(int) + 1)
+        if lat[0] * lat[1] * lat[2] > 4_000_000:
+            continue
+        cells = None if rng.random() < 0.5 else tuple(int(rng.integers(1, v)) for v in lat)
+        cases.append((lat, cells))
+    c = hpmc.default_constants()
+    rejected = 0
+    for lat, cells in cases:
+        t = torch.zeros((lat[2], lat[1], lat[0]), dtype=torch.float32, device=dev)
+        hp = hpmc.HistoPyramid(c)
+        hp.set_field_device(t)
+        if cells is not None:
+            hp.set_grid_size(*cells)
+        exp = oracle.layout(lat, cells)
+        try:
+            got = tuple(hp.layout())
+        except hpmc.HPMCError:
+            got = None
+            assert hp.last_error == _capi.ERR_LAYOUT, (lat, cells)
+        if exp is None:
+            rejected += 1
+            assert got is None, (lat, cells, got)
+        else:
+            assert got == exp.tile + exp.layout + (exp.size_l2, exp.size), (lat, cells, got)
+        hp.close()
+    assert rejected >= 5
+
+
 def test_caller_kernels_on_the_stream_stay_ordered(hpmc, oracle):
     """The build and extraction launch with programmatic stream serialization.
     A caller's kernel that rewrites the field right before a build, or the
