@@ -187,9 +187,10 @@ struct VertexCell {
     int k;
 };
 
-__device__ __forceinline__ void enter_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t key,
-                                            WarpBlock& B) {
-    descend(V, S, key, B.b, B.base, B.count);  // uniform across the warp
+// Block B.b with base B.base and count B.count found: load its active-cell
+// list and position the warp at block-relative vertex key - B.base.
+__device__ __forceinline__ void open_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t key,
+                                           WarpBlock& B) {
     B.nact = load_block(V, S, warp, lane, B.b);
     B.X0 = compact32(B.b) << 5;
     B.Y0 = compact32(B.b >> 1) << 5;
@@ -198,6 +199,30 @@ __device__ __forceinline__ void enter_block(const Volume& V, TraverseSmem& S, in
     const uint32_t k = key - B.base;
     B.cur = k == 0 ? 0u : find_active(S.act[warp], B.nact, k, lane);
     B.knext = k;
+}
+
+__device__ __forceinline__ void enter_block(const Volume& V, TraverseSmem& S, int warp, int lane, uint32_t key,
+                                            WarpBlock& B) {
+    descend(V, S, key, B.b, B.base, B.count);  // uniform across the warp
+    open_block(V, S, warp, lane, key, B);
+}
+
+// A warp walking forward out of block B.b: the next block with vertices, if
+// it lies among the next 32 level-5 entries (one coalesced load instead of a
+// descent through dependent loads).  The blocks in between hold no vertices,
+// so the next block's first vertex is B.base + B.count.  Entries of padding
+// blocks are zero: every level buffer is cleared when it is allocated and
+// only the generic classifier writes those entries (with zero).
+__device__ __forceinline__ bool next_sibling(const Volume& V, int lane, WarpBlock& B) {
+    const unsigned long long e = (unsigned long long)B.b + 1ull + (unsigned long long)lane;
+    const uint32_t c = e < (unsigned long long)V.nblocks ? __ldg(V.levels + V.level_off[kBlockLevel] + e) : 0u;
+    const uint32_t m = __ballot_sync(0xffffffffu, c != 0u);
+    if (m == 0u) return false;
+    const int i = __ffs(m) - 1;
+    B.base += B.count;
+    B.b += 1u + (uint32_t)i;
+    B.count = __shfl_sync(0xffffffffu, c, i);
+    return true;
 }
 
 // Steps 1-2 for one round of consecutive vertices (lane l holds vertex v,
@@ -214,7 +239,10 @@ __device__ __forceinline__ bool resolve_vertex(const Volume& V, TraverseSmem& S,
         const int leader = __ffs(pending) - 1;
         const uint32_t vl = __shfl_sync(0xffffffffu, v, leader);
         if (!B.have || vl < B.base || vl - B.base >= B.count) {
-            enter_block(V, S, warp, lane, vl, B);
+            if (B.have && vl - B.base == B.count && next_sibling(V, lane, B))
+                open_block(V, S, warp, lane, vl, B);
+            else
+                enter_block(V, S, warp, lane, vl, B);
         } else if (vl - B.base != B.knext) {
             B.cur = find_active(list, B.nact, vl - B.base, lane);
             B.knext = vl - B.base;
