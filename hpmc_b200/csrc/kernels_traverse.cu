@@ -12,7 +12,9 @@
 //      shared memory) to the 1024-key block, taking the first child whose
 //      running sum exceeds the key exactly as shadergen.cpp:448-467 does.  All
 //      lanes walk the same path, so every load is one broadcast transaction;
-//      consecutive vertices reuse the block and skip the descent.
+//      consecutive vertices reuse the block and skip the descent, and a warp
+//      that walks out of its block takes the next non-empty one from the
+//      following 32 level-5 entries (one coalesced load) when it lies there.
 //   2. in-block lookup (warp-cooperative; replaces the base-level steps of
 //      shadergen.cpp:469-495): on entering a block the warp turns its 1024
 //      codes into the list of active cells (count > 0) with their first
