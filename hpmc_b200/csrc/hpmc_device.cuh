@@ -125,15 +125,6 @@ __host__ __device__ __forceinline__ uint32_t morton_compact(uint64_t v) {
     v = (v | (v >> 16)) & 0x00000000ffffffffull;
     return (uint32_t)v;
 }
-__host__ __device__ __forceinline__ uint64_t morton_spread(uint64_t v) {
-    v &= 0xffffffffull;
-    v = (v | (v << 16)) & 0x0000ffff0000ffffull;
-    v = (v | (v << 8)) & 0x00ff00ff00ff00ffull;
-    v = (v | (v << 4)) & 0x0f0f0f0f0f0f0f0full;
-    v = (v | (v << 2)) & 0x3333333333333333ull;
-    v = (v | (v << 1)) & 0x5555555555555555ull;
-    return v;
-}
 // 16-bit value -> even bits of a 32-bit word
 __host__ __device__ __forceinline__ uint32_t morton_spread16(uint32_t v) {
     v &= 0xffffu;
