@@ -10,18 +10,24 @@ position/normal streams (HPMCextractVertices, vertex count read on the device).
            the field, build, count (host sync), extraction, D2H of every vertex;
            two volumes in flight (two handles on two streams: the H2D of
            volume k+1 overlaps volume k); the one-at-a-time figure beside it
-  roofline the build kernels (classify + reduce) against measured HBM copy
-           bandwidth; algorithmic bytes = field bytes read once
+  roofline the whole extraction step (classify + reduce + traverse) against
+           the measured HBM copy bandwidth; algorithmic bytes = field bytes
+           read once + 32 B per vertex written; the build and the traversal
+           alone are reported beside it ("kernels")
   cpu_baseline  the reference's generated shader passes run as C++ on the host
-           cores (the oracle restatement if they cannot be built), z-slab sample
+           cores (the oracle restatement if they cannot be built), full volume
   batched  64 uneven FP32 volumes: batched extractor (CUDA-graph replay) vs
-           the plain per-volume loop through the handle API, volumes/s
+           the plain per-volume loop through the handle API (sync-free: device
+           vertex counts, preallocated outputs; and the loop that reads every
+           count on the host), volumes/s
   adjoint  128^3 sphere SDF: adjoint (backward) time over forward time
 
 --impl reference times the reference's path on the host cores instead: the
 reference is GLSL for a GL driver (no GL stack on this box), so the shader
 text its generator emits is compiled for the CPU (oracle/glsl_pin.py, OpenMP
-over all host threads) and run on a z-slab of the workload.
+over all host threads) and run on the full 512^3 workload.  Its only normal
+estimate is the forward difference; the repository arm reports a
+forward-normal step beside its central-normal headline for that comparison.
 
 N > 1 (torchrun): every rank extracts its own volume (independent objects,
 no collective on the data path): weak scaling, value = all ranks' cells / max time.
@@ -47,11 +53,14 @@ WORKLOAD = ("cayley_512: FP32 512^3 lattice, Cayley cubic 16xyz+4(x^2+y^2+z^2)-1
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one build (classify_columns + reduce_levels)
-# per field byte, from ncu captures on the 384^3 Cayley field
-# (profiles/classify_columns_cayley384.txt, profiles/reduce_levels_cayley384.txt):
-# (226,560,000 + 8,833,024 + 1,067,264) / 226,492,416.  Traffic grows with
-# the field, so the 512^3 figure is this ratio times the field bytes.
+# per field byte, and of one traversal per vertex, from ncu captures on the
+# 384^3 Cayley field (226,492,416 field bytes, 2,092,962 vertices;
+# profiles/classify_columns_cayley384.txt, profiles/reduce_levels_cayley384.txt,
+# profiles/traverse_kernel_cayley384.txt).  Build traffic grows with the field
+# and traversal traffic with the vertices, so the 512^3 figure is these
+# ratios times the field bytes and the vertex count.
 BUILD_TRAFFIC_PER_FIELD_BYTE = (226560000 + 8833024 + 1067264) / 226492416
+TRAVERSE_TRAFFIC_PER_VERTEX = (27590000 + 14680000) / 2092962
 
 
 NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e nominal (DGX figure), reported beside the measured copy peak
@@ -126,82 +135,80 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _reference_slab(field_np, iso, slab, threads):
+def _reference_volume(field_np, iso, threads, max_vertices):
     """One run of the reference's own passes -- the GLSL its shader generator
-    emits, compiled for the CPU (oracle/glsl_pin.py) -- on a z-slab: base
-    level, reductions, count and extractVertex for every vertex.  Returns
-    (cells, vertices, threads)."""
+    emits, compiled for the CPU (oracle/glsl_pin.py) -- on the whole volume:
+    base level, reductions, count and extractVertex for every vertex (forward
+    normals, the reference's only estimate).  Returns (cells, vertices, threads)."""
     import os as _os
 
     from oracle import glsl_pin
 
-    sample = np.ascontiguousarray(field_np[: slab + 1])
     th = threads if threads > 0 else (_os.cpu_count() or 1)
-    _, n, _, _ = glsl_pin.run(sample, iso, max_vertices=1 << 22, keep_levels=False, threads=th)
-    cells = (sample.shape[2] - 1) * (sample.shape[1] - 1) * (sample.shape[0] - 1)
-    return cells, n, th
+    _, n, _, _ = glsl_pin.run(field_np, iso, max_vertices=max_vertices, keep_levels=False, threads=th)
+    fz, fy, fx = field_np.shape
+    return (fx - 1) * (fy - 1) * (fz - 1), n, th
 
 
-def cpu_baseline(field_np, iso, threads=0, min_seconds=10.0, slab=32):
+def cpu_baseline(field_np, iso, max_vertices, threads=0, min_seconds=10.0):
     """The reference's path on the host cores: its generated shaders run as C++
     (kind "reference"); the oracle restatement (kind "port") if they cannot be
-    built.  A z-slab of the workload (bounded sample), repeated >= min_seconds."""
+    built.  The whole workload, repeated for >= min_seconds."""
     from oracle import oracle as O
 
     try:
-        _reference_slab(field_np, iso, slab, threads)  # compile + warm
+        _reference_volume(field_np, iso, threads, max_vertices)  # compile + warm
         kind = "reference"
     except Exception:
         kind = "port"
-    sample = np.ascontiguousarray(field_np[: slab + 1])
-    cells = (sample.shape[2] - 1) * (sample.shape[1] - 1) * (sample.shape[0] - 1)
+    fz, fy, fx = field_np.shape
+    cells = (fx - 1) * (fy - 1) * (fz - 1)
     t0 = time.perf_counter()
     runs = 0
     verts = 0
     cores = threads if threads > 0 else O.max_threads()
     while True:
         if kind == "reference":
-            _, verts, cores = _reference_slab(field_np, iso, slab, threads)
+            _, verts, cores = _reference_volume(field_np, iso, threads, max_vertices)
         else:
-            verts, _, _ = O.extract_count(sample, iso, normal_mode=O.NORMALS_CENTRAL, threads=threads, geometry=True)
+            verts, _, _ = O.extract_count(field_np, iso, normal_mode=O.NORMALS_FORWARD, threads=threads,
+                                          geometry=True)
         runs += 1
         if time.perf_counter() - t0 >= min_seconds:
             break
     dt = time.perf_counter() - t0
     what = ("the reference's generated GLSL passes compiled for the CPU (base level, reductions, count, "
             "extractVertex with forward normals)" if kind == "reference"
-            else "oracle restatement (codes+pyramid+traversal+FP64 geometry)")
+            else "oracle restatement (codes+pyramid+traversal+FP64 geometry, forward normals)")
     return {"value": cells * runs / dt / 1e9, "unit": "Gcells/s", "cores": cores, "kind": kind,
-            "sample": f"z-slab {sample.shape[2]}x{sample.shape[1]}x{sample.shape[0]} of the 512^3 field "
-                      f"({cells} cells, {verts} vertices), {what}, {runs} runs"}
+            "sample": f"the whole {fx}x{fy}x{fz} workload ({cells} cells, {verts} vertices), {what}, {runs} runs"}
 
 
 def run_reference(args, rank, world):
     """The reference's path on the host cores (rank 0 only): its generated
-    shaders compiled for the CPU, all host threads, one 512x512x33 z-slab of
-    the workload per step."""
+    shaders compiled for the CPU, all host threads, the whole 512^3 workload
+    per step."""
     if rank != 0:
         return
     from hpmc_b200 import datasets
 
-    field, iso = datasets.cayley(512)
-    slab = 32
+    field, iso = datasets.cayley(args.lattice)
+    max_vertices = 1 << 23 if args.lattice <= 512 else 1 << 26
     try:
         for _ in range(args.warmup):
-            cells, verts, threads = _reference_slab(field, iso, slab, 0)
+            cells, verts, threads = _reference_volume(field, iso, 0, max_vertices)
         kind = "reference"
-        step = lambda: _reference_slab(field, iso, slab, 0)  # noqa: E731
+        step = lambda: _reference_volume(field, iso, 0, max_vertices)  # noqa: E731
     except Exception:
         from oracle import oracle as O
 
         kind = "port"
-        sample = np.ascontiguousarray(field[: slab + 1])
         threads = O.max_threads()
-        cells = 511 * 511 * slab
+        fz, fy, fx = field.shape
 
         def step():
-            n, _, _ = O.extract_count(sample, iso, normal_mode=O.NORMALS_CENTRAL, threads=threads, geometry=True)
-            return cells, n, threads
+            n, _, _ = O.extract_count(field, iso, normal_mode=O.NORMALS_FORWARD, threads=threads, geometry=True)
+            return (fx - 1) * (fy - 1) * (fz - 1), n, threads
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -210,26 +217,31 @@ def run_reference(args, rank, world):
         vals.append(cells / (time.perf_counter() - s0) / 1e9)
     dt = time.perf_counter() - t0
     value = statistics.median(vals)
-    sample = (f"z-slab 512x512x{slab + 1} of the 512^3 field per step ({cells} cells, {verts} vertices): "
+    sample = (f"the whole {args.lattice}^3 workload per step ({cells} cells, {verts} vertices): "
               + ("the reference's generated GLSL passes compiled for the CPU (forward normals)" if kind == "reference"
-                 else "oracle restatement"))
+                 else "oracle restatement (forward normals)"))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Gcells/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "lattice": [512, 512, 512]},
+            "data": "synthetic", "config": {"workload": WORKLOAD, "lattice": [args.lattice] * 3},
             "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference runs its passes as GLSL in a GL driver, unavailable on this box (no GL stack); "
-                    "its generated shader text is compiled and run on the host cores instead"}
+                    "its generated shader text is compiled and run on the host cores instead. Its only normal "
+                    "estimate is the forward difference (the repository arm's forward_normals_step_ms is the "
+                    "like-for-like figure)"}
     print(json.dumps(line), flush=True)
 
 
 def run_batched(args, dev, stream, rank=0, world=1):
     """64 uneven FP32 metaball volumes: one CUDA-graph replay of the batched
-    extractor vs the plain per-volume loop through the handle API (build,
-    acquire count, extract), both on the same stream, CUDA events.  With N
-    ranks each takes its share of the 64 volumes (greedy split by cells) and
-    the time is the maximum over the ranks."""
+    extractor vs the plain per-volume loop through the handle API, both on the
+    same stream, CUDA events.  Two plain loops: the sync-free one (build, then
+    HPMCextractVerticesToBuffers reading the vertex count on the device, into
+    outputs allocated beforehand) and the one that reads every count on the
+    host (build, acquire count, extract).  With N ranks each takes its share
+    of the 64 volumes (greedy split by cells) and the time is the maximum
+    over the ranks."""
     import torch
     import torch.distributed as dist
 
@@ -263,26 +275,35 @@ def run_batched(args, dev, stream, rank=0, world=1):
             outs.append(n)
     total = sum(outs)
 
-    def plain():
+    def plain_sync():
         for hp, th, iso in zip(hps, ths, isos):
             hp.build(iso)
             hp.acquire_number_of_vertices()
             th.extract()
 
+    def plain():  # sync-free: device counts, outputs sized beforehand
+        for hp, th, iso, (p, q), n in zip(hps, ths, isos, bufs, outs):
+            hp.build(iso)
+            th.extract_to(p, q, n, sync=False)
+
+    bufs = [th._keep["buf"] for th in ths]
     steps = max(3, min(args.steps, 20))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        for _ in range(3):
-            plain()
-        stream.synchronize()
-        if world > 1:
-            dist.barrier()
-        e0.record(stream)
-        for _ in range(steps):
-            plain()
-        e1.record(stream)
-        stream.synchronize()
-    plain_ms = multi.max_over_ranks(e0.elapsed_time(e1) / steps, device=dev)
+    loop_ms = {}
+    for name, fn in (("sync_free", plain), ("host_sync", plain_sync)):
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                fn()
+            stream.synchronize()
+            if world > 1:
+                dist.barrier()
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+        loop_ms[name] = multi.max_over_ranks(e0.elapsed_time(e1) / steps, device=dev)
+    plain_ms = loop_ms["sync_free"]
 
     b = H.Batch(tensors, isos, normals=H.NORMALS_CENTRAL)
     pos = torch.empty((total, 4), dtype=torch.float32, device=dev)
@@ -313,9 +334,14 @@ def run_batched(args, dev, stream, rank=0, world=1):
                         "central normals",
             "volumes": nall, "cells": cells_all, "field_bytes": sum(f.nbytes for f, _ in all_vols),
             "vertices": int(multi.sum_over_ranks(total, device=dev)), "ranks": world,
-            "plain_ms": plain_ms, "batched_ms": batched_ms,
+            "plain_ms": plain_ms, "plain_host_sync_ms": loop_ms["host_sync"], "batched_ms": batched_ms,
             "plain_vols_per_s": nall / (plain_ms * 1e-3), "batched_vols_per_s": nall / (batched_ms * 1e-3),
-            "speedup": plain_ms / batched_ms, "batched_gcells_per_s": cells_all / (batched_ms * 1e-3) / 1e9,
+            "speedup": plain_ms / batched_ms, "speedup_vs_host_sync_loop": loop_ms["host_sync"] / batched_ms,
+            "plain_loop": "sync-free: per volume HPMCbuildHistopyramid + HPMCextractVerticesToBuffers "
+                          "(device vertex count, outputs allocated beforehand)",
+            "batched_gcells_per_s": cells_all / (batched_ms * 1e-3) / 1e9,
+            "batched_hbm_fraction": (sum(f.nbytes for f, _ in all_vols) + 32 * total) / (batched_ms * 1e-3) / 1e9
+            / hbm_peak()[0],
             "tuning": {"column_slices": tuning[0], "traverse_ctas_per_sm": tuning[1], "rounds": tuning[2]},
             "graph": True, "steps": steps}
 
@@ -450,6 +476,24 @@ def run_hpmc(args, rank, world, local_rank):
     clocks.stop()
     build_ms = [ev[3 * i].elapsed_time(ev[3 * i + 1]) for i in range(args.steps)]
     trav_ms = [ev[3 * i + 1].elapsed_time(ev[3 * i + 2]) for i in range(args.steps)]
+    # --- the same step with forward normals (the reference's only estimate),
+    # timed like the headline loop, for the like-for-like comparison with the
+    # reference arm
+    hp.set_normal_mode(H.NORMALS_FORWARD)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            step()
+    torch.cuda.synchronize()
+    f_begin = torch.cuda.Event(enable_timing=True)
+    f_end = torch.cuda.Event(enable_timing=True)
+    f_begin.record(stream)
+    for _ in range(args.steps):
+        step()
+    f_end.record(stream)
+    stream.synchronize()
+    fwd_ms = multi.max_over_ranks(f_begin.elapsed_time(f_end) / args.steps, device=dev)
+    hp.set_normal_mode(H.NORMALS_CENTRAL)
+
     total_ms = multi.max_over_ranks(total_ms, device=dev)
     ms_per_step = total_ms / args.steps
     value = cells * world * args.steps / (total_ms * 1e-3) / 1e9
@@ -459,15 +503,29 @@ def run_hpmc(args, rank, world, local_rank):
     trav_avg = statistics.mean(trav_ms)
     out_bytes = 32 * nverts
     alg_bytes = field_bytes + out_bytes
-    roof = {"kernel": "build = classify_columns + reduce_levels (classify dominates)",
-            "bound": "hbm", "achieved": field_bytes / (build_avg * 1e-3) / 1e9, "peak": peak,
-            "unit": "GB/s", "frac": field_bytes / (build_avg * 1e-3) / 1e9 / peak,
-            "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes,
-            "traffic_source": "ncu dram__bytes_read+write of the 384^3 capture, scaled by field bytes",
-            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": field_bytes,
-            "avg_launch_ms": build_avg,
-            "timing": "CUDA events around every build of a second pass of K steps on the launching stream",
-            "frac_of_nominal": field_bytes / (build_avg * 1e-3) / 1e9 / NOMINAL_HBM_GBS}
+    gbs = lambda nbytes, ms: nbytes / (ms * 1e-3) / 1e9  # noqa: E731
+    roof = {"kernel": "whole extraction step = classify_columns + reduce_levels + traverse_kernel "
+                      "(three programmatically dependent launches)",
+            "bound": "hbm", "achieved": gbs(alg_bytes, ms_per_step), "peak": peak, "unit": "GB/s",
+            "frac": gbs(alg_bytes, ms_per_step) / peak,
+            "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes + TRAVERSE_TRAFFIC_PER_VERTEX * nverts,
+            "traffic_source": "ncu dram__bytes_read+write of the 384^3 captures of the three kernels, scaled by "
+                              "field bytes (build) and vertices (traversal)",
+            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
+            "algorithmic_bytes": "field bytes read once + 32 B per vertex (float4 position + float4 normal)",
+            "avg_launch_ms": ms_per_step,
+            "timing": "CUDA events at the ends of K back-to-back steps on the launching stream",
+            "frac_of_nominal": gbs(alg_bytes, ms_per_step) / NOMINAL_HBM_GBS}
+    kernels = {
+        "build": {"kernels": "classify_columns + reduce_levels", "ms": build_avg,
+                  "algorithmic_bytes": field_bytes, "achieved_gbs": gbs(field_bytes, build_avg),
+                  "frac": gbs(field_bytes, build_avg) / peak,
+                  "traffic": BUILD_TRAFFIC_PER_FIELD_BYTE * field_bytes},
+        "traverse": {"kernels": "traverse_kernel", "ms": trav_avg, "algorithmic_bytes": out_bytes,
+                     "achieved_gbs": gbs(out_bytes, trav_avg), "frac": gbs(out_bytes, trav_avg) / peak,
+                     "traffic": TRAVERSE_TRAFFIC_PER_VERTEX * nverts},
+        "timing": "CUDA events around every build and extraction of a second pass of K steps",
+    }
     step_frac = alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak
 
     # --- e2e through the public API with host buffers ----------------------
@@ -566,7 +624,7 @@ def run_hpmc(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(field_np, iso)
+        cpu = cpu_baseline(field_np, iso, max_vertices=max(nverts, 1))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
@@ -579,6 +637,9 @@ def run_hpmc(args, rank, world, local_rank):
                            "normals": "central", "l2": "inputs larger than L2 (537 MB field per step)",
                            "parallelism": f"replicas x{world} (independent volumes)"},
                 "roofline": roof,
+                "kernels": kernels,
+                "forward_normals_step_ms": fwd_ms,
+                "forward_normals_value": cells * world / (fwd_ms * 1e-3) / 1e9,
                 "step_hbm_fraction": step_frac,
                 "step_hbm_fraction_of_nominal": alg_bytes / (ms_per_step * 1e-3) / 1e9 / NOMINAL_HBM_GBS,
                 "step_algorithmic_bytes": alg_bytes,
@@ -588,6 +649,7 @@ def run_hpmc(args, rank, world, local_rank):
                 "batched": batched,
                 "adjoint": adjoint,
                 "gpu_launches": 3 * args.steps,
+                "gpu_launches_note": "classify + reduce + traverse per timed step (headline loop)",
                 "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
     th.close()

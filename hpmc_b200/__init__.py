@@ -14,12 +14,13 @@ from __future__ import annotations
 import ctypes as C
 
 from . import _capi
-from ._capi import (NORMALS_CENTRAL, NORMALS_FORWARD, SCALAR_F32, SCALAR_U8,  # noqa: F401
+from ._capi import (NORMALS_CENTRAL, NORMALS_FORWARD, SCALAR_F32, SCALAR_F32X4, SCALAR_U8,  # noqa: F401
                     SCALAR_UNORM8, STATUS_NAMES)
 
 __all__ = [
     "Constants", "HistoPyramid", "TraversalHandle", "Batch", "HPMCError", "extract", "lib",
-    "NORMALS_FORWARD", "NORMALS_CENTRAL", "SCALAR_F32", "SCALAR_U8", "SCALAR_UNORM8",
+    "register_device_field", "unregister_device_field",
+    "NORMALS_FORWARD", "NORMALS_CENTRAL", "SCALAR_F32", "SCALAR_U8", "SCALAR_UNORM8", "SCALAR_F32X4",
 ]
 
 
@@ -45,11 +46,41 @@ def _ptr(t) -> int | None:
 def _scalar_type(t, unorm: bool) -> int:
     import torch
 
+    if t.dtype == torch.float32 and t.dim() == 4 and t.shape[3] == 4:
+        return SCALAR_F32X4  # (z, y, x, 4): gradient x, y, z and the value, a GL RGBA float texture
     if t.dtype == torch.float32:
         return SCALAR_F32
     if t.dtype == torch.uint8:
         return SCALAR_UNORM8 if unorm else SCALAR_U8
     raise TypeError(f"unsupported field dtype {t.dtype} (float32 or uint8)")
+
+
+def _field_layout(field) -> None:
+    if not field.is_cuda:
+        raise ValueError("field must be a CUDA tensor")
+    if field.dim() == 4:
+        if field.shape[3] != 4 or field.stride(3) != 1 or field.stride(2) != 4:
+            raise ValueError("a (z, y, x, 4) field must be contiguous along x and its 4 channels")
+    elif field.stride(2) != 1:
+        raise ValueError("field must have unit stride along x")
+
+
+def register_device_field(field, unorm: bool = False) -> int:
+    """HPMCregisterDeviceField: a name for a (z, y, x) or (z, y, x, 4) CUDA
+    tensor, the stand-in for a GL 3-D texture name (HPMCsetFieldTexture3D).
+    The tensor must outlive its use."""
+    _field_layout(field)
+    es = field.element_size()
+    fz, fy, fx = field.shape[:3]
+    name = lib().HPMCregisterDeviceField(field.data_ptr(), _scalar_type(field, unorm), fx, fy, fz,
+                                         field.stride(1) * es, field.stride(0) * es)
+    if not name:
+        raise HPMCError(_capi.ERR_INVALID_VALUE, "HPMCregisterDeviceField")
+    return int(name)
+
+
+def unregister_device_field(name: int) -> None:
+    lib().HPMCunregisterDeviceField(int(name))
 
 
 class Constants:
@@ -119,14 +150,12 @@ class HistoPyramid:
         return int(lib().HPMCgetLastError(self.ptr))
 
     def set_field_device(self, field, unorm: bool = False):
-        """Field tensor (z, y, x), float32 or uint8, on the current CUDA device."""
-        if not field.is_cuda:
-            raise ValueError("field must be a CUDA tensor")
+        """Field tensor (z, y, x) float32 or uint8, or (z, y, x, 4) float32
+        (gradient + value), on the current CUDA device."""
+        _field_layout(field)
         es = field.element_size()
-        if field.stride(2) != 1:
-            raise ValueError("field must have unit stride along x")
         self._keep["field"] = field
-        fz, fy, fx = field.shape
+        fz, fy, fx = field.shape[:3]
         self.set_lattice_size(fx, fy, fz)
         _check(lib().HPMCsetFieldDevice(self.ptr, field.data_ptr(), _scalar_type(field, unorm),
                                         field.stride(1) * es, field.stride(0) * es), "HPMCsetFieldDevice")
@@ -175,6 +204,11 @@ class HistoPyramid:
         s = C.c_uint(0)
         _check(lib().HPMCgetDeviceStatus(self.ptr, C.byref(s)), "HPMCgetDeviceStatus")
         return int(s.value)
+
+    def set_test_stall(self, box: int, wait_limit_us: int = 0):
+        """Failure-detection test hook (HPMCsetTestStall): classifier box `box`
+        never arrives, so the build times out; box < 0 turns it off."""
+        _check(lib().HPMCsetTestStall(self.ptr, int(box), int(wait_limit_us)), "HPMCsetTestStall")
 
     def close(self):
         if self.ptr:
@@ -318,6 +352,11 @@ class Batch:
         if st != _capi.OK and not (allow_truncation and st == _capi.ERR_CAPACITY):
             raise HPMCError(st, "HPMCbatchGetOffsets")
         return [int(v) for v in out]
+
+    def set_test_stall(self, volume: int, box: int, wait_limit_us: int = 0):
+        """Failure-detection test hook (HPMCbatchSetTestStall)."""
+        _check(lib().HPMCbatchSetTestStall(self.ptr, int(volume), int(box), int(wait_limit_us)),
+               "HPMCbatchSetTestStall")
 
     def autotune(self, pos, nrm, capacity: int | None = None, stream=None):
         import torch

@@ -29,12 +29,12 @@ ERR_NO_FIELD = 10
 ERR_OVERFLOW = 11
 ERR_TIMEOUT = 12
 ERR_TOO_LARGE = 13
-STATIC_SCRATCH_BYTES = 4 << 20
+STATIC_SCRATCH_BYTES = 16 << 20
 
 STATUS_NAMES = {v: k for k, v in globals().items() if k.startswith("ERR_") or k == "OK"}
 
 # HPMCScalarType
-SCALAR_F32, SCALAR_U8, SCALAR_UNORM8 = 0, 1, 2
+SCALAR_F32, SCALAR_U8, SCALAR_UNORM8, SCALAR_F32X4 = 0, 1, 2, 3
 # HPMCNormalMode
 NORMALS_FORWARD, NORMALS_CENTRAL = 0, 1
 
@@ -82,8 +82,11 @@ _SIGS = {
     "HPMCsetTraversalDebugBuffers": (C.c_int, [vp, vp, vp]),
     "HPMCgetDeviceStatus": (C.c_int, [vp, C.POINTER(C.c_uint)]),
     "HPMCgetClassifyPath": (C.c_int, [vp, C.POINTER(C.c_int)]),
+    "HPMCsetTestStall": (C.c_int, [vp, C.c_int, C.c_uint]),
+    "HPMCregisterFieldFunctor": (C.c_int, [C.c_char_p, vp]),
+    "HPMCunregisterFieldFunctor": (C.c_int, [C.c_char_p]),
     "HPMCextractStatic": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_size_t, C.c_float,
-                                    C.c_int, C.POINTER(C.c_float), vp, vp, C.c_size_t, vp, vp]),
+                                    C.c_int, C.POINTER(C.c_float), vp, vp, C.c_size_t, vp, vp, vp]),
     "HPMCextractVerticesIndexed": (C.c_int, [vp, vp, vp, C.c_size_t, vp, C.c_size_t, C.POINTER(C.c_uint64),
                                              C.POINTER(C.c_uint64)]),
     # batched extraction
@@ -97,6 +100,7 @@ _SIGS = {
     "HPMCbatchSetTuning": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     "HPMCbatchGetTuning": (C.c_int, [vp, C.POINTER(C.c_int)]),
     "HPMCbatchAutotune": (C.c_int, [vp, vp, vp, C.c_size_t, vp, C.POINTER(C.c_int)]),
+    "HPMCbatchSetTestStall": (C.c_int, [vp, C.c_int, C.c_int, C.c_uint]),
 }
 
 

@@ -2,8 +2,10 @@
 
 Steps:
   1. import HPMC's case tables (``csrc/gen_tables.py``) from the HPMC source
-     tree named by ``HPMC_SRC`` (default: the tree this repository was built
-     against) into ``csrc/_gen/hpmc_case_tables.h``;
+     tree named by the ``HPMC_SRC`` environment variable (default: an HPMC
+     checkout named ``reference`` beside this repository) into
+     ``csrc/_gen/hpmc_case_tables.h`` (git-ignored; a prebuilt header is used
+     when no tree is found);
   2. compile every ``csrc/*.cu`` with nvcc for ``sm_100a`` and link one shared
      library exposing the C ABI of ``include/hpmc.h``.
 
@@ -24,7 +26,8 @@ GEN = os.path.join(CSRC, "_gen", "hpmc_case_tables.h")
 OUT_DIR = os.path.join(PKG, "_lib")
 OBJ_DIR = os.path.join(OUT_DIR, "obj")
 LIB = os.path.join(OUT_DIR, "libhpmc_b200.so")
-DEFAULT_HPMC_SRC = "/root/reference"
+# The HPMC source tree: $HPMC_SRC, else a checkout named `reference` beside the repository.
+DEFAULT_HPMC_SRC = os.path.normpath(os.path.join(ROOT, os.pardir, "reference"))
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -99,7 +102,7 @@ def build(verbose_ptxas: bool = False) -> str:
 
 APPS_DIR = os.path.join(PKG, "apps")
 APPS_OUT = os.path.join(OUT_DIR, "apps")
-APPS = ["texture3d", "cayley", "metaballs", "transform_feedback"]
+APPS = ["texture3d", "cayley", "metaballs", "transform_feedback", "custom_functor"]
 
 
 def app_path(name: str) -> str:
@@ -115,13 +118,20 @@ def build_apps() -> list[str]:
     cuda = os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
     out = []
     for name in APPS:
-        src = os.path.join(APPS_DIR, name + ".cpp")
+        cu = os.path.join(APPS_DIR, name + ".cu")
+        src = cu if os.path.exists(cu) else os.path.join(APPS_DIR, name + ".cpp")
         dst = app_path(name)
         deps = [src, os.path.join(APPS_DIR, "app_common.hpp"), os.path.join(ROOT, "include", "hpmc.h"), lib]
+        if src == cu:  # a caller with device code of its own (include/hpmc_functor.cuh)
+            deps += [os.path.join(ROOT, "include", "hpmc_functor.cuh")] + _headers()
         if not os.path.exists(dst) or os.path.getmtime(dst) < max(os.path.getmtime(d) for d in deps):
-            cmd = [cxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(cuda, "include"),
-                   src, "-o", dst, "-L" + OUT_DIR, "-lhpmc_b200", "-L" + os.path.join(cuda, "lib64"), "-lcudart",
-                   "-Wl,-rpath,$ORIGIN/.."]
+            if src == cu:
+                cmd = [nvcc(), *NVCC_FLAGS, src, "-o", dst, "-L" + OUT_DIR, "-lhpmc_b200",
+                       "-Xlinker", "-rpath,$ORIGIN/.."]
+            else:
+                cmd = [cxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                       "-I" + os.path.join(cuda, "include"), src, "-o", dst, "-L" + OUT_DIR, "-lhpmc_b200",
+                       "-L" + os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN/.."]
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"app build failed for {name}:\n{r.stdout}\n{r.stderr}")

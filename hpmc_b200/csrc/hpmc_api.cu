@@ -22,6 +22,7 @@
 #include "hpmc.h"
 #include "hpmc_device.cuh"
 #include "hpmc_fetch.cuh"
+#include "hpmc_geometry.cuh"
 #include "hpmc_host.h"
 #include "hpmc_kernels.h"
 
@@ -46,9 +47,12 @@ std::mutex g_fields_mu;
 std::map<GLuint, FieldDesc> g_fields;
 GLuint g_next_field = 1;
 
+// Caller-registered field functors (HPMCregisterFieldFunctor), by name.
+std::mutex g_functors_mu;
+std::map<std::string, HPMCFieldFunctorOps> g_functors;
+
 using hpmc::host::determine_layout;  // init.cpp:72-149
 using hpmc::host::elem_size;
-using hpmc::host::tensor_map_encoder;
 
 }  // namespace
 
@@ -66,6 +70,8 @@ struct HPMCHistoPyramid {
     enum { kNone, kArray, kFunctor } fmode = kNone;
     FieldDesc field;
     hpmc::FunctorParams functor{};
+    bool user_functor = false;          // functor.id == 0: the caller's registered functor below
+    HPMCFieldFunctorOps user_ops{};
     bool gradient = false;
     int normal_mode = HPMC_NORMALS_FORWARD;
     cudaStream_t stream = nullptr;
@@ -85,6 +91,9 @@ struct HPMCHistoPyramid {
     float threshold = 0.f;
     unsigned long long count_cached = 0;
     bool count_valid = false;
+    // test hook (HPMCsetTestStall): a classifier box that never arrives
+    int test_stall_box = -1;
+    unsigned long long test_wait_ns = hpmc::kWaitLimitNs;
 };
 
 struct HPMCTraversalHandle {
@@ -126,15 +135,18 @@ void release_device(HPMCHistoPyramid* h) {
 int bind_field(HPMCHistoPyramid* h) {
     Volume& V = h->V;
     if (h->fmode == HPMCHistoPyramid::kFunctor) {
-        V.ftype = hpmc::kFieldFunctor;
+        V.ftype = h->user_functor ? hpmc::kFieldUser : hpmc::kFieldFunctor;
         V.field = nullptr;
         V.row_pitch = V.slice_pitch = 0;
         V.functor = h->functor;
-        V.gradient = (h->gradient && hpmc::functor_has_gradient(h->functor.id)) ? 1 : 0;
+        const bool has_grad = h->user_functor ? h->user_ops.has_gradient != 0
+                                              : hpmc::functor_has_gradient(h->functor.id);
+        V.gradient = (h->gradient && has_grad) ? 1 : 0;
+        h->have_tmap = false;
         return HPMC_OK;
     }
-    V.gradient = 0;
     if (h->fmode != HPMCHistoPyramid::kArray || !h->field.ptr) return HPMC_ERR_NO_FIELD;
+    V.gradient = h->gradient ? 1 : 0;
     const FieldDesc& f = h->field;
     const size_t es = elem_size(f.type);
     const size_t rp = f.row_pitch ? f.row_pitch : (size_t)h->lattice[0] * es;
@@ -142,36 +154,24 @@ int bind_field(HPMCHistoPyramid* h) {
     if (rp % es || sp % es || rp < (size_t)h->lattice[0] * es || sp < rp * (size_t)h->lattice[1])
         return HPMC_ERR_INVALID_VALUE;
     V.field = f.ptr;
-    V.ftype = f.type == HPMC_SCALAR_F32 ? hpmc::kFieldF32
-              : f.type == HPMC_SCALAR_U8 ? hpmc::kFieldU8
-                                         : hpmc::kFieldUNorm8;
+    V.ftype = hpmc::host::field_type(f.type);
     V.row_pitch = (long long)(rp / es);
     V.slice_pitch = (long long)(sp / es);
     V.idx32 = (V.slice_pitch * ((long long)h->lattice[2] + 1) < (1ll << 31)) ? 1 : 0;
     // TMA column path: column layout, 16-byte aligned base and pitches
-    h->have_tmap = false;
-    if (V.column_layout && ((uintptr_t)f.ptr % 16 == 0) && rp % 16 == 0 && sp % 16 == 0) {
-        auto enc = tensor_map_encoder();
-        if (enc) {
-            const cuuint64_t dims[3] = {(cuuint64_t)h->lattice[0], (cuuint64_t)h->lattice[1],
-                                        (cuuint64_t)h->lattice[2]};
-            const cuuint64_t strides[2] = {(cuuint64_t)rp, (cuuint64_t)sp};
-            const bool f32 = f.type == HPMC_SCALAR_F32;
-            // one ring stage of the column kernel: 32+1 columns padded to a
-            // 16-byte row, 32+1 rows, kLayersPerBox layers
-            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, (cuuint32_t)hpmc::kLayersPerBox};
-            const cuuint32_t estr[3] = {1, 1, 1};
-            CUresult r = enc(&h->tmap, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
-                             const_cast<void*>(f.ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            h->have_tmap = (r == CUDA_SUCCESS);
-        }
-    }
+    // (scalar fields only: a float4 field takes the generic classifier)
+    h->have_tmap = V.column_layout && f.type != HPMC_SCALAR_F32X4 && ((uintptr_t)f.ptr % 16 == 0) &&
+                   rp % 16 == 0 && sp % 16 == 0 &&
+                   hpmc::host::encode_column_map(&h->tmap, f.ptr, f.type, h->lattice, rp, sp);
     return HPMC_OK;
 }
 
 // HPMCsetup (init.cpp:48-69): layout + device memory for it.
+//
+// Everything the device sees is ordered on the handle's stream: buffers are
+// cleared with stream-ordered memsets (work still in flight on the stream --
+// an extraction reading the levels and the work queue -- finishes first), and
+// buffers that must grow are freed only after the stream has drained.
 bool setup(HPMCHistoPyramid* h) {
     if (!h->tainted) return true;
     int L[6];
@@ -182,61 +182,19 @@ bool setup(HPMCHistoPyramid* h) {
     std::memcpy(h->layout, L, sizeof L);
     Volume& V = h->V;
     V = Volume{};
-    for (int i = 0; i < 3; i++) {
-        V.lattice[i] = h->lattice[i];
-        V.cells[i] = h->cells[i];
-        V.scale[i] = h->extent[i] / (float)h->cells[i];
-        V.dscale[i] = (double)h->extent[i] / (double)h->cells[i];
-    }
-    V.tile_x = L[0];
-    V.tile_y = L[1];
-    V.layout_x = L[2];
-    V.layout_y = L[3];
-    V.size_l2 = L[4];
-    auto ilog2 = [](int v) {
-        int e = 0;
-        while ((1 << e) < v) e++;
-        return e;
-    };
-    V.wx_l2 = ilog2(2 * L[0]);
-    V.wy_l2 = ilog2(2 * L[1]);
-    V.lx_l2 = ilog2(L[2]);
-    V.jtop = std::max(hpmc::kBlockLevel, V.size_l2 + 1);
-    // dense levels, top first, each padded to a multiple of 4 entries
-    long long off = 0;
-    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
-        V.level_off[j] = off;
-        off += (hpmc::level_entries(V.size_l2, j) + 3) & ~3ll;
-    }
-    const long long levels_total = off;
-    V.nblocks = hpmc::level_entries(V.size_l2, hpmc::kBlockLevel);
-    V.top_cached = 0;
-    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
-        const long long end = V.level_off[j] + ((hpmc::level_entries(V.size_l2, j) + 3) & ~3ll);
-        if (end > hpmc::kTopCacheEntries) break;
-        V.top_cached = (int)end;
-    }
-    V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
-    V.nfx = (V.cells[0] + 31) / 32;
-    V.nfy = (V.cells[1] + 31) / 32;
-    // slices per column: the longest column that still gives the persistent
-    // classifier (2 CTAs per SM) ~12 columns per CTA
-    {
-        const long long target = 24ll * h->constants->num_sms;
-        V.column_slices = hpmc::kColumnSliceChoices[3];
-        for (int zc : hpmc::kColumnSliceChoices) {
-            if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= target) {
-                V.column_slices = zc;
-                break;
-            }
-        }
-    }
-    const long long slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
+    long long levels_total = 0, slots = 0;
+    hpmc::host::volume_layout(V, h->lattice, h->cells, h->extent, L, &levels_total, &slots);
+    V.column_slices = hpmc::host::default_column_slices(V, h->constants->num_sms);
     // (re)allocate
     if ((size_t)levels_total > h->levels_cap || (size_t)slots > h->arena_cap || !h->d_ctrl) {
+        if (h->d_ctrl && cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            cudaGetLastError();
+            h->status = HPMC_ERR_CUDA;
+            return false;
+        }
         release_device(h);
         if (cudaMalloc(&h->d_levels, sizeof(uint32_t) * levels_total) != cudaSuccess ||
-            cudaMalloc(&h->d_arena, sizeof(uint32_t) * hpmc::kBlockWords * (size_t)slots) != cudaSuccess ||
+            cudaMalloc(&h->d_arena, hpmc::kSlotBytes * (size_t)slots) != cudaSuccess ||
             cudaMalloc(&h->d_ctrl, sizeof(Ctrl)) != cudaSuccess) {
             cudaGetLastError();
             release_device(h);
@@ -246,8 +204,9 @@ bool setup(HPMCHistoPyramid* h) {
         h->levels_cap = (size_t)levels_total;
         h->arena_cap = (size_t)slots;
     }
-    if (cudaMemset(h->d_ctrl, 0, sizeof(Ctrl)) != cudaSuccess ||
-        cudaMemset(h->d_levels, 0, sizeof(uint32_t) * levels_total) != cudaSuccess) {
+    if (cudaMemsetAsync(h->d_ctrl, 0, sizeof(Ctrl), h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->d_levels, 0, sizeof(uint32_t) * levels_total, h->stream) != cudaSuccess) {
+        cudaGetLastError();
         h->status = HPMC_ERR_CUDA;
         return false;
     }
@@ -284,8 +243,18 @@ int launch_extract(HPMCTraversalHandle* th, float* pos, float* nrm, float* feedb
     O.dbg_cell = reinterpret_cast<int4*>(th->dbg_cell);
     O.dbg_t = th->dbg_t;
     if (h->count_valid && h->count_cached > cap) h->status = HPMC_ERR_CAPACITY;
-    cudaError_t e = hpmc::launch_traverse(h->V, O, h->normal_mode, traverse_grid(h), h->stream);
+    cudaError_t e;
+    if (h->V.ftype == hpmc::kFieldUser) {
+        // the caller's instantiation of the traversal (include/hpmc_functor.cuh)
+        const int mode = h->binary ? hpmc::kGeomBinary
+                                   : (h->normal_mode == HPMC_NORMALS_CENTRAL ? hpmc::kGeomCentral : hpmc::kGeomForward);
+        e = h->user_ops.traverse(&h->V, &O, mode, traverse_grid(h), h->stream) == HPMC_OK ? cudaSuccess
+                                                                                       : cudaErrorLaunchFailure;
+    } else {
+        e = hpmc::launch_traverse(h->V, O, h->normal_mode, traverse_grid(h), h->stream);
+    }
     if (e != cudaSuccess) {
+        cudaGetLastError();
         set_error(h, HPMC_ERR_CUDA, true);
         return HPMC_ERR_CUDA;
     }
@@ -377,10 +346,6 @@ void HPMCsetGridExtent(HPMCHistoPyramid* h, GLfloat x, GLfloat y, GLfloat z) {
 
 void HPMCsetFieldTexture3D(HPMCHistoPyramid* h, GLuint texture, GLboolean gradient) {
     if (!valid(h)) return;
-    if (gradient) {
-        set_error(h, HPMC_ERR_UNSUPPORTED, true);
-        return;
-    }
     FieldDesc f;
     {
         std::lock_guard<std::mutex> lk(g_fields_mu);
@@ -391,10 +356,13 @@ void HPMCsetFieldTexture3D(HPMCHistoPyramid* h, GLuint texture, GLboolean gradie
         }
         f = it->second;
     }
+    // The layout and the device buffers do not depend on the field (it is
+    // bound at every build), so a new field does not taint the handle -- as
+    // in the reference, where only a change of fetch mode does
+    // (hpiface.cpp:164-184).
     h->fmode = HPMCHistoPyramid::kArray;
     h->field = f;
-    h->gradient = false;
-    h->tainted = true;
+    h->gradient = gradient != 0;
     h->broken = false;
     h->status = HPMC_OK;
 }
@@ -403,30 +371,42 @@ void HPMCsetFieldCustom(HPMCHistoPyramid* h, const char* src, GLuint builder_tex
     (void)builder_texunit;
     if (!valid(h)) return;
     int id = 0;
+    bool user = false;
+    HPMCFieldFunctorOps ops{};
     if (src) {
         const std::string s(src);
         if (s == "hpmc:cayley") id = 1;
         else if (s == "hpmc:metaballs") id = 2;
         else if (s == "hpmc:twist_metaballs") id = 3;
         else if (s == "hpmc:spheres") id = 4;
+        else {
+            std::lock_guard<std::mutex> lk(g_functors_mu);
+            auto it = g_functors.find(s);
+            if (it != g_functors.end()) {
+                user = true;
+                ops = it->second;
+            }
+        }
     }
-    if (!id) {
+    if (!id && !user) {
         set_error(h, HPMC_ERR_UNSUPPORTED, true);
         return;
     }
     h->fmode = HPMCHistoPyramid::kFunctor;
     h->functor = hpmc::FunctorParams{};
     h->functor.id = id;
+    h->user_functor = user;
+    h->user_ops = ops;
     h->gradient = gradient != 0;
-    h->tainted = true;
-    h->broken = false;
+    h->broken = false;  // the field is bound at every build: no taint
     h->status = HPMC_OK;
 }
 
 GLuint HPMCgetBuilderProgram(HPMCHistoPyramid* h) {
     if (!valid(h) || h->broken) return 0;
     if (h->tainted && !setup(h)) return 0;
-    return h->fmode == HPMCHistoPyramid::kFunctor ? 0x100u + (GLuint)h->functor.id : 0u;
+    if (h->fmode != HPMCHistoPyramid::kFunctor) return 0u;
+    return h->user_functor ? 0x200u : 0x100u + (GLuint)h->functor.id;
 }
 
 void HPMCdestroyHandle(HPMCHistoPyramid* h) {
@@ -450,20 +430,20 @@ void HPMCbuildHistopyramid(HPMCHistoPyramid* h, GLfloat threshold) {
     V.iso = threshold;
     V.binary = h->binary ? 1 : 0;
     // uint8 fields: f(b) is monotonic in b, so f(b) < iso  <=>  b < u8_thr
-    // (host float division is IEEE, the same rounding as the device's)
-    {
-        const float thr = h->binary ? 0.5f : threshold;
-        int n = 0;
-        for (int b = 0; b < 256; b++) {
-            const float f = (V.ftype == hpmc::kFieldUNorm8) ? (float)b / 255.0f : (float)b;
-            if (f < thr) n = b + 1;
-        }
-        V.u8_thr = n;
-    }
+    V.u8_thr = hpmc::host::u8_threshold(V.ftype, h->binary ? 0.5f : threshold);
     V.codes_out = h->codes_capture;
+    V.stall_box = h->test_stall_box;
+    V.wait_limit_ns = h->test_wait_ns;
     h->threshold = threshold;
     const int max_ctas = h->constants->num_sms * 16;
-    cudaError_t e = hpmc::launch_classify(V, h->have_tmap ? &h->tmap : nullptr, max_ctas, h->stream);
+    cudaError_t e;
+    if (V.ftype == hpmc::kFieldUser) {
+        // the caller's instantiation of the generic classifier (include/hpmc_functor.cuh)
+        const int grid = (int)std::min<long long>(V.nblocks, (long long)max_ctas);
+        e = h->user_ops.classify(&V, grid, h->stream) == HPMC_OK ? cudaSuccess : cudaErrorLaunchFailure;
+    } else {
+        e = hpmc::launch_classify(V, h->have_tmap ? &h->tmap : nullptr, max_ctas, h->stream);
+    }
     if (e == cudaSuccess) e = hpmc::launch_reduce(V, h->stream);
     if (e != cudaSuccess) {
         set_error(h, HPMC_ERR_CUDA, true);  // hpiface.cpp:263-266
@@ -482,6 +462,11 @@ GLuint HPMCacquireNumberOfVertices(HPMCHistoPyramid* h) {
             cudaMemcpy(&c, h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost) != cudaSuccess) {
             set_error(h, HPMC_ERR_CUDA, true);
             return 0;
+        }
+        if (c.status & (hpmc::kStatusTimeout | hpmc::kStatusOverflow)) {
+            // reported once: the next build starts from a clean status word
+            // (the handle may be un-broken by a setter that does not taint)
+            cudaMemsetAsync(&h->d_ctrl->status, 0, sizeof(unsigned int), h->stream);
         }
         if (c.status & hpmc::kStatusTimeout) {
             set_error(h, HPMC_ERR_TIMEOUT, true);
@@ -550,7 +535,8 @@ int HPMCgetLastError(HPMCHistoPyramid* h) { return valid(h) ? h->status : HPMC_E
 
 GLuint HPMCregisterDeviceField(const void* ptr, int type, GLsizei x, GLsizei y, GLsizei z, size_t row_pitch,
                                size_t slice_pitch) {
-    if (!ptr || x < 1 || y < 1 || z < 1 || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_UNORM8) return 0;
+    if (!ptr || x < 1 || y < 1 || z < 1 || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_F32X4) return 0;
+    if (type == HPMC_SCALAR_F32X4 && (uintptr_t)ptr % 16) return 0;
     FieldDesc f;
     f.ptr = ptr;
     f.type = type;
@@ -572,7 +558,8 @@ void HPMCunregisterDeviceField(GLuint name) {
 
 int HPMCsetFieldDevice(HPMCHistoPyramid* h, const void* ptr, int type, size_t row_pitch, size_t slice_pitch) {
     if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
-    if (!ptr || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_UNORM8) {
+    if (!ptr || type < HPMC_SCALAR_F32 || type > HPMC_SCALAR_F32X4 ||
+        (type == HPMC_SCALAR_F32X4 && (uintptr_t)ptr % 16)) {
         h->status = HPMC_ERR_INVALID_VALUE;
         return h->status;
     }
@@ -583,8 +570,7 @@ int HPMCsetFieldDevice(HPMCHistoPyramid* h, const void* ptr, int type, size_t ro
     h->field.row_pitch = row_pitch;
     h->field.slice_pitch = slice_pitch;
     h->gradient = false;
-    h->tainted = true;
-    h->broken = false;
+    h->broken = false;  // the field is bound at every build: no taint
     h->status = HPMC_OK;
     return HPMC_OK;
 }
@@ -665,7 +651,9 @@ int HPMCextractVerticesAdjoint(HPMCTraversalHandle* th, const float* dpos, const
     if (h->broken) return HPMC_ERR_BROKEN;
     if (!h->built) return HPMC_ERR_NOT_BUILT;
     if (!dfield || (dpos && (uintptr_t)dpos % 16) || (dnrm && (uintptr_t)dnrm % 16)) return HPMC_ERR_INVALID_VALUE;
-    if (h->V.ftype == hpmc::kFieldFunctor) return HPMC_ERR_UNSUPPORTED;
+    if (h->V.ftype == hpmc::kFieldFunctor || h->V.ftype == hpmc::kFieldUser || h->V.ftype == hpmc::kFieldF32X4 ||
+        h->V.gradient)
+        return HPMC_ERR_UNSUPPORTED;
     if (h->binary) return HPMC_OK;  // midpoints and table normals: no dependence on f
     hpmc::AdjointIO A{};
     A.dpos = reinterpret_cast<const float4*>(dpos);
@@ -689,6 +677,7 @@ int HPMCextractVerticesIndexed(HPMCTraversalHandle* th, float* positions, float*
     if ((positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16) ||
         (indices && (uintptr_t)indices % 4))
         return HPMC_ERR_INVALID_VALUE;
+    if (h->V.ftype == hpmc::kFieldUser) return HPMC_ERR_UNSUPPORTED;  // its kernels live in the caller's code
     const GLuint n = HPMCacquireNumberOfVertices(h);  // sizes the scratch (host sync)
     if (n == 0 && h->status != HPMC_OK) return h->status;
     // scratch: keys | table keys | first | scan | table vals | tile sums | meta | unique count
@@ -746,6 +735,22 @@ int HPMCextractVerticesIndexed(HPMCTraversalHandle* th, float* positions, float*
     return (unique > vertex_capacity || (size_t)n > index_capacity) ? HPMC_ERR_CAPACITY : HPMC_OK;
 }
 
+int HPMCregisterFieldFunctor(const char* name, const HPMCFieldFunctorOps* ops) {
+    if (!name || !*name || std::strncmp(name, "hpmc:", 5) == 0 || !ops || ops->abi != HPMC_FIELD_FUNCTOR_ABI ||
+        ops->volume_bytes != (int)sizeof(Volume) || ops->outputs_bytes != (int)sizeof(hpmc::TraverseOut) ||
+        !ops->classify || !ops->traverse)
+        return HPMC_ERR_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(g_functors_mu);
+    g_functors[name] = *ops;
+    return HPMC_OK;
+}
+
+int HPMCunregisterFieldFunctor(const char* name) {
+    if (!name) return HPMC_ERR_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(g_functors_mu);
+    return g_functors.erase(name) ? HPMC_OK : HPMC_ERR_INVALID_VALUE;
+}
+
 int HPMCsetCodeCapture(HPMCHistoPyramid* h, uint8_t* device_codes) {
     if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
     h->codes_capture = device_codes;
@@ -786,6 +791,13 @@ int HPMCsetTraversalDebugBuffers(HPMCTraversalHandle* th, int32_t* cell_info, fl
     if (cell_info && (uintptr_t)cell_info % 16) return HPMC_ERR_INVALID_VALUE;
     th->dbg_cell = cell_info;
     th->dbg_t = t;
+    return HPMC_OK;
+}
+
+int HPMCsetTestStall(HPMCHistoPyramid* h, int box, unsigned int wait_limit_us) {
+    if (!valid(h)) return HPMC_ERR_INVALID_HANDLE;
+    h->test_stall_box = box < 0 ? -1 : box;
+    h->test_wait_ns = wait_limit_us ? 1000ull * wait_limit_us : hpmc::kWaitLimitNs;
     return HPMC_OK;
 }
 
@@ -879,10 +891,11 @@ extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_s
                                  GLsizei z_size, size_t row_pitch_bytes, size_t slice_pitch_bytes, GLfloat iso,
                                  int normal_mode, const GLfloat* extent, float* positions, float* normals,
                                  size_t capacity_vertices, unsigned int* device_vertex_count,
-                                 void* cuda_stream) {
+                                 unsigned int* device_status, void* cuda_stream) {
     if (!field || !device_vertex_count || scalar_type < HPMC_SCALAR_F32 || scalar_type > HPMC_SCALAR_UNORM8 ||
         (normal_mode != HPMC_NORMALS_FORWARD && normal_mode != HPMC_NORMALS_CENTRAL) ||
-        (positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16))
+        (positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16) ||
+        ((uintptr_t)device_vertex_count % 4) || (device_status && (uintptr_t)device_status % 4))
         return HPMC_ERR_INVALID_VALUE;
     const int lattice[3] = {x_size, y_size, z_size};
     const int cells[3] = {x_size - 1, y_size - 1, z_size - 1};
@@ -894,56 +907,15 @@ extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_s
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
 
     Volume V{};
-    for (int i = 0; i < 3; i++) {
-        V.lattice[i] = lattice[i];
-        V.cells[i] = cells[i];
-        const float e = extent ? extent[i] : 1.0f;
-        V.scale[i] = e / (float)cells[i];
-        V.dscale[i] = (double)e / (double)cells[i];
-    }
-    V.tile_x = L[0];
-    V.tile_y = L[1];
-    V.layout_x = L[2];
-    V.layout_y = L[3];
-    V.size_l2 = L[4];
-    auto ilog2 = [](int v) {
-        int e = 0;
-        while ((1 << e) < v) e++;
-        return e;
-    };
-    V.wx_l2 = ilog2(2 * L[0]);
-    V.wy_l2 = ilog2(2 * L[1]);
-    V.lx_l2 = ilog2(L[2]);
-    V.jtop = std::max(hpmc::kBlockLevel, V.size_l2 + 1);
-    long long off = 0;
-    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
-        V.level_off[j] = off;
-        off += (hpmc::level_entries(V.size_l2, j) + 3) & ~3ll;
-    }
-    const long long level_entries_total = off;
-    V.nblocks = hpmc::level_entries(V.size_l2, hpmc::kBlockLevel);
-    V.top_cached = 0;
-    for (int j = V.jtop; j >= hpmc::kBlockLevel; j--) {
-        const long long end = V.level_off[j] + ((hpmc::level_entries(V.size_l2, j) + 3) & ~3ll);
-        if (end > hpmc::kTopCacheEntries) break;
-        V.top_cached = (int)end;
-    }
-    V.column_layout = (2 * V.tile_x >= 32 && 2 * V.tile_y >= 32) ? 1 : 0;
-    V.nfx = (V.cells[0] + 31) / 32;
-    V.nfy = (V.cells[1] + 31) / 32;
-    V.column_slices = hpmc::kColumnSliceChoices[3];
-    for (int zc : hpmc::kColumnSliceChoices) {
-        if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= 12ll * dev->num_sms) {
-            V.column_slices = zc;
-            break;
-        }
-    }
-    const long long slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
+    const float ext[3] = {extent ? extent[0] : 1.0f, extent ? extent[1] : 1.0f, extent ? extent[2] : 1.0f};
+    long long level_entries_total = 0, slots = 0;
+    hpmc::host::volume_layout(V, lattice, cells, ext, L, &level_entries_total, &slots);
+    V.column_slices = hpmc::host::default_column_slices(V, dev->num_sms);
 
-    // carve the scratch: control block | dense levels | code arena
+    // carve the scratch: control block | dense levels | active-cell lists
     const size_t ctrl_bytes = align256(sizeof(Ctrl));
     const size_t levels_bytes = align256(sizeof(uint32_t) * (size_t)level_entries_total);
-    const size_t arena_bytes = sizeof(uint32_t) * hpmc::kBlockWords * (size_t)slots;
+    const size_t arena_bytes = hpmc::kSlotBytes * (size_t)slots;
     if (ctrl_bytes + levels_bytes + arena_bytes > (size_t)HPMC_STATIC_SCRATCH_BYTES) return HPMC_ERR_TOO_LARGE;
     unsigned char* base = dev->scratch;
     V.ctrl = reinterpret_cast<Ctrl*>(base);
@@ -958,38 +930,16 @@ extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_s
     if (rp % es || sp % es || rp < (size_t)lattice[0] * es || sp < rp * (size_t)lattice[1])
         return HPMC_ERR_INVALID_VALUE;
     V.field = field;
-    V.ftype = scalar_type == HPMC_SCALAR_F32 ? hpmc::kFieldF32
-              : scalar_type == HPMC_SCALAR_U8 ? hpmc::kFieldU8
-                                              : hpmc::kFieldUNorm8;
+    V.ftype = hpmc::host::field_type(scalar_type);
     V.row_pitch = (long long)(rp / es);
     V.slice_pitch = (long long)(sp / es);
     V.idx32 = (V.slice_pitch * ((long long)lattice[2] + 1) < (1ll << 31)) ? 1 : 0;
     V.iso = iso;
     V.binary = 0;
-    {
-        int n = 0;
-        for (int b = 0; b < 256; b++) {
-            const float f = (V.ftype == hpmc::kFieldUNorm8) ? (float)b / 255.0f : (float)b;
-            if (f < iso) n = b + 1;
-        }
-        V.u8_thr = n;
-    }
+    V.u8_thr = hpmc::host::u8_threshold(V.ftype, iso);
     CUtensorMap tmap;
-    bool have_tmap = false;
-    if (V.column_layout && ((uintptr_t)field % 16 == 0) && rp % 16 == 0 && sp % 16 == 0) {
-        auto enc = tensor_map_encoder();
-        if (enc) {
-            const cuuint64_t dims[3] = {(cuuint64_t)lattice[0], (cuuint64_t)lattice[1], (cuuint64_t)lattice[2]};
-            const cuuint64_t strides[2] = {(cuuint64_t)rp, (cuuint64_t)sp};
-            const bool f32 = scalar_type == HPMC_SCALAR_F32;
-            const cuuint32_t box[3] = {f32 ? 36u : 48u, 33u, (cuuint32_t)hpmc::kLayersPerBox};
-            const cuuint32_t estr[3] = {1, 1, 1};
-            have_tmap = enc(&tmap, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3,
-                            const_cast<void*>(field), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-        }
-    }
+    const bool have_tmap = V.column_layout && ((uintptr_t)field % 16 == 0) && rp % 16 == 0 && sp % 16 == 0 &&
+                           hpmc::host::encode_column_map(&tmap, field, scalar_type, lattice, rp, sp);
 
     // the array keeps the previous call's contents: clear the control block
     // (counters, status) and the dense levels (padding entries read as zero)
@@ -1003,10 +953,13 @@ extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_s
         O.capacity = capacity_vertices;
         e = hpmc::launch_traverse(V, O, normal_mode, dev->num_sms * dev->traverse_ctas_per_sm, stream);
     }
-    // full vertex count (little-endian low word of the 64-bit total)
+    // full vertex count (little-endian low word of the 64-bit total) and the
+    // device status bits of this call (the next call clears them)
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(device_vertex_count, &V.ctrl->total, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
                             stream);
+    if (e == cudaSuccess && device_status)
+        e = cudaMemcpyAsync(device_status, &V.ctrl->status, sizeof(unsigned int), cudaMemcpyDeviceToDevice, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return HPMC_ERR_CUDA;

@@ -7,7 +7,7 @@
 // Device memory of a batch (one allocation):
 //   batch control block | per-volume control blocks | descriptors |
 //   tensor maps | brick, reduce-chunk and work-item prefix arrays |
-//   output offsets | dense levels of every volume | code arenas
+//   output offsets | dense levels of every volume | active-cell list arenas
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -331,7 +331,7 @@ int HPMCcreateBatch(HPMCConstants* c, const HPMCBatchVolume* volumes, int count,
     const size_t o_vbase = off;
     off = align_up(off + sizeof(unsigned long long) * (count + 1), 256);
     const size_t o_arena = off;
-    off += sizeof(uint32_t) * hpmc::kBlockWords * (size_t)arena_total;
+    off += hpmc::kSlotBytes * (size_t)arena_total;
     if (cudaMalloc(&b->d_base, off) != cudaSuccess) {
         cudaGetLastError();
         delete b;
@@ -357,7 +357,7 @@ int HPMCcreateBatch(HPMCConstants* c, const HPMCBatchVolume* volumes, int count,
     for (int v = 0; v < count; v++) {
         Volume& V = b->hv[v];
         V.levels = d_levels + lev_off[v];
-        V.arena = d_arena + (size_t)hpmc::kBlockWords * (size_t)arena_off[v];
+        V.arena = d_arena + (size_t)hpmc::kSlotWords * (size_t)arena_off[v];
         V.arena_slots = (v + 1 < count ? arena_off[v + 1] : arena_total) - arena_off[v];
         V.ctrl = b->d_ctrls + v;
     }
@@ -415,6 +415,17 @@ int HPMCbatchGetTuning(HPMCBatch* b, int out[3]) {
     return HPMC_OK;
 }
 
+int HPMCbatchSetTestStall(HPMCBatch* b, int volume, int box, unsigned int wait_limit_us) {
+    if (!valid(b)) return HPMC_ERR_INVALID_HANDLE;
+    if (volume < 0 || volume >= b->nvol) return HPMC_ERR_INVALID_VALUE;
+    for (int v = 0; v < b->nvol; v++) {
+        b->hv[v].stall_box = (v == volume && box >= 0) ? box : -1;
+        b->hv[v].wait_limit_ns = wait_limit_us ? 1000ull * wait_limit_us : hpmc::kWaitLimitNs;
+    }
+    b->upload = true;
+    return HPMC_OK;
+}
+
 int HPMCbatchExtract(HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices, void* cuda_stream) {
     if (!valid(b)) return HPMC_ERR_INVALID_HANDLE;
     if ((positions && (uintptr_t)positions % 16) || (normals && (uintptr_t)normals % 16))
@@ -440,23 +451,24 @@ int HPMCbatchGetOffsets(HPMCBatch* b, unsigned long long* host_offsets) {
         cudaGetLastError();
         return HPMC_ERR_CUDA;
     }
+    // timeouts of the column classifier and overflows are recorded per volume
+    std::vector<Ctrl> cs(b->nvol);
+    if (cudaMemcpy(cs.data(), b->d_ctrls, sizeof(Ctrl) * b->nvol, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return HPMC_ERR_CUDA;
+    }
     unsigned int st = bc.status;
-    if (!(st & hpmc::kStatusTimeout)) {
-        // timeouts of the column classifier are recorded per volume
-        std::vector<Ctrl> cs(b->nvol);
-        if (cudaMemcpy(cs.data(), b->d_ctrls, sizeof(Ctrl) * b->nvol, cudaMemcpyDeviceToHost) != cudaSuccess) {
-            cudaGetLastError();
-            return HPMC_ERR_CUDA;
-        }
-        for (const Ctrl& c : cs) st |= c.status;
+    for (const Ctrl& c : cs) st |= c.status;
+    if (st) {
+        // every status bit is reported once: clear them for the next extraction
+        const unsigned int clear = 0;
+        cudaMemcpy(&b->d_bctrl->status, &clear, sizeof clear, cudaMemcpyHostToDevice);
+        for (int v = 0; v < b->nvol; v++)
+            if (cs[v].status) cudaMemcpy(&b->d_ctrls[v].status, &clear, sizeof clear, cudaMemcpyHostToDevice);
     }
     if (st & hpmc::kStatusTimeout) return HPMC_ERR_TIMEOUT;
     if (st & hpmc::kStatusOverflow) return HPMC_ERR_OVERFLOW;
-    if (st & hpmc::kStatusCapacity) {
-        const unsigned int clear = 0;
-        cudaMemcpy(&b->d_bctrl->status, &clear, sizeof clear, cudaMemcpyHostToDevice);
-        return HPMC_ERR_CAPACITY;
-    }
+    if (st & hpmc::kStatusCapacity) return HPMC_ERR_CAPACITY;
     return HPMC_OK;
 }
 

@@ -17,6 +17,10 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kLayersPerBox = 8;
 constexpr int kRingStages = 2;
 constexpr int kColumnSliceChoices[4] = {63, 31, 15, 7};
+// Columns per SM the single-volume column classifier aims for when it picks
+// the column depth: 2 resident CTAs per SM with ~12 columns each, so that
+// the persistent CTAs end evenly (fewer, longer columns measured slower).
+constexpr int kColumnsPerSm = 24;
 
 // Traversal: top pyramid entries cached in shared memory per CTA
 // (levels with <= 1024 entries: 1 + 4 + ... + 1024, each padded to 4).

@@ -15,10 +15,12 @@
 //     count as uint32 -- level j equals the reference's mip level j flattened
 //     channel by channel (level j texel t, channel c <-> entry 4*morton(t)+c);
 //   * below block level nothing is stored densely: each block with a non-zero
-//     count gets a 1 KiB "arena" slot holding its 1024 MC codes in Morton
-//     order (4 codes per uint32 word), from which the traversal recomputes
-//     the per-cell counts.  Levels 0..4 of the reference are thus implied by
-//     the codes; codes of empty blocks are all 0 or 255 and are not needed.
+//     count gets an "arena" slot holding its active-cell list -- the cells
+//     with vertices, in Morton (= vertex) order, each with its MC code and the
+//     block-relative index of its first vertex.  Levels 0..4 of the reference
+//     are thus implied by the lists: the count of a Morton range of cells is
+//     the difference of two list starts.  Cells of empty blocks are all
+//     inside or all outside and are not needed.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -29,15 +31,33 @@ namespace hpmc {
 
 constexpr int kBlockLevel = 5;       // 4^5 keys per block
 constexpr int kBlockKeys = 1024;
-constexpr int kBlockWords = 256;     // arena words per block (4 codes / word)
 constexpr int kMaxLevels = 40;
+
+// Active-cell list of one block (one arena slot): one word per cell with
+// vertices, in Morton order,
+//     start << 18 | code << 10 | cell
+// start = block-relative index of the cell's first vertex (< 15 * 1024),
+// code = MC case, cell = Morton index of the cell in the block.  The last
+// entry is followed by kListSentinels words of all ones (start 16383, past
+// any vertex), so a warp may read the 32 entries after any list position
+// without knowing the list's length.
+constexpr int kListSentinels = 32;
+constexpr int kSlotWords = kBlockKeys + kListSentinels;
+constexpr size_t kSlotBytes = sizeof(uint32_t) * (size_t)kSlotWords;
+constexpr uint32_t kListSentinel = 0xffffffffu;
+constexpr int kListStartShift = 18;
 
 enum FieldType : int {
     kFieldF32 = 0,      // float
     kFieldU8 = 1,       // uint8 read as float(b)
     kFieldUNorm8 = 2,   // uint8 read as b/255 (GL_ALPHA UNSIGNED_BYTE texture)
     kFieldFunctor = 3,  // registered device functor evaluated at texel centres
+    kFieldF32X4 = 4,    // float4 (gradient x, y, z, value): a GL RGBA float texture
+    kFieldUser = 5,     // a caller's functor type (include/hpmc_functor.cuh), a template argument
 };
+
+// Template argument of the kernels when the field is not a caller's functor.
+struct NoUserField {};
 
 enum NormalMode : int {
     kNormalsForward = 0,  // reference default: iso - lerp(f(a+e), f(b+e), t)
@@ -83,7 +103,9 @@ struct Volume {
     int cells[3];
     float iso;
     int binary;
-    int gradient;            // functor field with analytic gradient normals (HPMC_fetchGrad)
+    int gradient;            // gradient normals: a functor's analytic gradient (HPMC_fetchGrad) or the
+                             // .xyz of an RGBA field (shadergen.cpp:260-266, 539-551); scalar
+                             // fields read a zero gradient there, as GL's alpha textures do
     float scale[3];          // extent / cells
     double dscale[3];        // extent / cells in FP64 (geometry)
     // layout (init.cpp:72-149); all sizes are powers of two
@@ -105,7 +127,7 @@ struct Volume {
     int column_layout;
     int nfx, nfy;                      // 32-cell footprints per slice in x, y
     int column_slices;                 // slices per column CTA
-    uint32_t* arena;                   // kBlockWords words per slot
+    uint32_t* arena;                   // kSlotWords words (one active-cell list) per slot
     long long arena_slots;             // capacity of the arena
     Ctrl* ctrl;
     // optional capture of every cell's code, [cz][cy][cx] (inspection)
@@ -113,6 +135,14 @@ struct Volume {
     // custom field
     FunctorParams functor;
     unsigned long long vertex_base;    // first output index of this volume (batched)
+    // bounded waits of the column classifier (kWaitLimitNs unless a test lowers it)
+    unsigned long long wait_limit_ns;
+    // Test hook (failure detection without a fault): the column classifier's
+    // producer never issues box `stall_box` of its first column (no expect_tx,
+    // no copy), so the consumers' bounded waits run out and the build reports
+    // kStatusTimeout.  -1: off.
+    int stall_box;
+    int pad_;
 };
 
 // --- Morton helpers (X on even bits) ---------------------------------------

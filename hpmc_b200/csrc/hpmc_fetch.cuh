@@ -4,7 +4,10 @@
 // with apps/texture3d/texture3d.cpp:135-139): NEAREST sampling at texel
 // centres with GL_CLAMP, i.e. clamp-to-edge integer indexing.  uint8 arrays
 // read either as float(b) (kFieldU8) or as GL's normalised b/255
-// (kFieldUNorm8, a GL_ALPHA/GL_UNSIGNED_BYTE texture).
+// (kFieldUNorm8, a GL_ALPHA/GL_UNSIGNED_BYTE texture).  float4 arrays
+// (kFieldF32X4) hold a GL RGBA float texture: the field is the alpha (value)
+// channel, and the gradient-mode traversal reads .xyz as the gradient
+// (shadergen.cpp:260-266).
 //
 // Functor fields replace the reference's custom GLSL fetch snippet
 // (HPMCsetFieldCustom, hpiface.cpp:187-200; shadergen.cpp:270-286): the
@@ -126,6 +129,8 @@ template <int FT>
 __device__ __forceinline__ float fetch_raw(const Volume& V, long long off) {
     if constexpr (FT == kFieldF32) {
         return __ldg(static_cast<const float*>(V.field) + off);
+    } else if constexpr (FT == kFieldF32X4) {
+        return __ldg(static_cast<const float*>(V.field) + 4 * off + 3);
     } else if constexpr (FT == kFieldU8) {
         return u8_to_float(__ldg(static_cast<const unsigned char*>(V.field) + off));
     } else {
@@ -134,17 +139,30 @@ __device__ __forceinline__ float fetch_raw(const Volume& V, long long off) {
 }
 
 // f(x,y,z) with the reference's addressing; x,y,z may lie outside the lattice.
-template <int FT>
+// UF: the caller's functor type when FT == kFieldUser (include/hpmc_functor.cuh).
+template <int FT, class UF = NoUserField>
 __device__ __forceinline__ float fetch(const Volume& V, int x, int y, int z) {
     if constexpr (FT == kFieldFunctor) {
         return functor_value(V.functor, texel_centre(x, V.lattice[0]), texel_centre(y, V.lattice[1]),
                              texel_centre(z, V.lattice[2]));
+    } else if constexpr (FT == kFieldUser) {
+        return UF::value(V.functor.p, V.functor.count, texel_centre(x, V.lattice[0]),
+                         texel_centre(y, V.lattice[1]), texel_centre(z, V.lattice[2]));
     } else {
         x = min(max(x, 0), V.lattice[0] - 1);
         y = min(max(y, 0), V.lattice[1] - 1);
         z = min(max(z, 0), V.lattice[2] - 1);
         return fetch_raw<FT>(V, (long long)z * V.slice_pitch + (long long)y * V.row_pitch + x);
     }
+}
+
+// The whole RGBA sample (gradient x, y, z, value) of a float4 field, with the
+// reference's clamp-to-edge addressing.
+__device__ __forceinline__ float4 fetch_rgba(const Volume& V, int x, int y, int z) {
+    x = min(max(x, 0), V.lattice[0] - 1);
+    y = min(max(y, 0), V.lattice[1] - 1);
+    z = min(max(z, 0), V.lattice[2] - 1);
+    return __ldg(static_cast<const float4*>(V.field) + ((long long)z * V.slice_pitch + (long long)y * V.row_pitch + x));
 }
 
 }  // namespace hpmc

@@ -72,21 +72,24 @@ struct EdgeField {
     float am[3], bm[3];  // f(a - e_i), f(b - e_i)   (central differences only)
 };
 
-template <int FT, bool CENTRAL>
+template <int FT, bool CENTRAL, class UF = NoUserField>
 __device__ __forceinline__ void gather_edge(const Volume& V, const int* a, int axis, int cx, int cy, int cz,
                                             EdgeField& F) {
     const int ex = axis == 0, ey = axis == 1, ez = axis == 2;
+    constexpr bool kArray = FT != kFieldFunctor && FT != kFieldUser;
     // samples span cell-1 .. cell+3 on each axis
-    const bool interior = FT != kFieldFunctor && cx >= 1 && cx <= V.lattice[0] - 4 && cy >= 1 &&
-                          cy <= V.lattice[1] - 4 && cz >= 1 && cz <= V.lattice[2] - 4;
-    if (FT != kFieldFunctor && interior && V.idx32) {
+    const bool interior = kArray && cx >= 1 && cx <= V.lattice[0] - 4 && cy >= 1 && cy <= V.lattice[1] - 4 &&
+                          cz >= 1 && cz <= V.lattice[2] - 4;
+    if (kArray && interior && V.idx32) {
         // 32-bit element offsets from the sample at a (one wide address each)
-        using T = typename std::conditional<FT == kFieldF32, float, unsigned char>::type;
+        using T = typename std::conditional<
+            FT == kFieldF32, float, typename std::conditional<FT == kFieldF32X4, float4, unsigned char>::type>::type;
         const int o[3] = {1, (int)V.row_pitch, (int)V.slice_pitch};
         const T* pa = static_cast<const T*>(V.field) + (a[2] * o[2] + a[1] * o[1] + a[0]);
         const T* pb = pa + (axis == 0 ? o[0] : axis == 1 ? o[1] : o[2]);
         auto ld = [](const T* p) -> float {
             if constexpr (FT == kFieldF32) return __ldg(p);
+            else if constexpr (FT == kFieldF32X4) return __ldg(&p->w);
             else if constexpr (FT == kFieldU8) return u8_to_float(__ldg(p));
             else return unorm8_to_float(__ldg(p));
         };
@@ -101,7 +104,7 @@ __device__ __forceinline__ void gather_edge(const Volume& V, const int* a, int a
                 F.bm[i] = ld(pb - o[i]);
             }
         }
-    } else if (FT != kFieldFunctor && interior) {
+    } else if (kArray && interior) {
         const long long o[3] = {1ll, V.row_pitch, V.slice_pitch};
         const long long pa = (long long)a[2] * V.slice_pitch + (long long)a[1] * V.row_pitch + a[0];
         const long long pb = pa + (axis == 0 ? o[0] : axis == 1 ? o[1] : o[2]);
@@ -117,16 +120,16 @@ __device__ __forceinline__ void gather_edge(const Volume& V, const int* a, int a
             }
         }
     } else {
-        F.va = fetch<FT>(V, a[0], a[1], a[2]);
-        F.vb = fetch<FT>(V, a[0] + ex, a[1] + ey, a[2] + ez);
+        F.va = fetch<FT, UF>(V, a[0], a[1], a[2]);
+        F.vb = fetch<FT, UF>(V, a[0] + ex, a[1] + ey, a[2] + ez);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             const int dx = i == 0, dy = i == 1, dz = i == 2;
-            F.ap[i] = fetch<FT>(V, a[0] + dx, a[1] + dy, a[2] + dz);
-            F.bp[i] = fetch<FT>(V, a[0] + ex + dx, a[1] + ey + dy, a[2] + ez + dz);
+            F.ap[i] = fetch<FT, UF>(V, a[0] + dx, a[1] + dy, a[2] + dz);
+            F.bp[i] = fetch<FT, UF>(V, a[0] + ex + dx, a[1] + ey + dy, a[2] + ez + dz);
             if (CENTRAL) {
-                F.am[i] = fetch<FT>(V, a[0] - dx, a[1] - dy, a[2] - dz);
-                F.bm[i] = fetch<FT>(V, a[0] + ex - dx, a[1] + ey - dy, a[2] + ez - dz);
+                F.am[i] = fetch<FT, UF>(V, a[0] - dx, a[1] - dy, a[2] - dz);
+                F.bm[i] = fetch<FT, UF>(V, a[0] + ex - dx, a[1] + ey - dy, a[2] + ez - dz);
             }
         }
     }
@@ -144,7 +147,7 @@ enum { kGeomForward = 0, kGeomCentral = 1, kGeomBinary = 2 };
 // A_i, B_i the end-point differences).  Its rounding error is bounded by
 // 7u sqrt(sum_i (|A_i|+|B_i|)^2), u = 2^-24; when that bound exceeds 2e-6 of
 // |n| (a normal that nearly cancels) the vertex is recomputed in float-float.
-template <int FT, int MODE>
+template <int FT, int MODE, class UF = NoUserField>
 __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int axis, int cx, int cy, int cz,
                                             const float* binary_normal, float p[3], float n[3], float& t_out) {
     float t;
@@ -153,20 +156,44 @@ __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int a
         n[0] = binary_normal[0];
         n[1] = binary_normal[1];
         n[2] = binary_normal[2];
-    } else if (FT == kFieldFunctor && V.gradient) {
-        // analytic gradient (shadergen.cpp:539-551): t from the functor values
-        // at a and b; forward mode keeps the reference's n = iso - lerp(grad a,
-        // grad b, t), central mode gives -lerp(grad a, grad b, t)
-        const float pa[3] = {texel_centre(a[0], V.lattice[0]), texel_centre(a[1], V.lattice[1]),
-                             texel_centre(a[2], V.lattice[2])};
+    } else if (V.gradient) {
+        // gradient mode (shadergen.cpp:539-551): t from the values at a and b,
+        // the gradients from HPMC_fetchGrad -- a functor's analytic gradient or
+        // the .xyz of an RGBA field (single-channel fields read zero there, as
+        // GL's alpha textures do); forward mode keeps the reference's
+        // n = iso - lerp(grad a, grad b, t), central mode gives -lerp(grad a, grad b, t)
         const int b[3] = {a[0] + (axis == 0), a[1] + (axis == 1), a[2] + (axis == 2)};
-        const float pb[3] = {texel_centre(b[0], V.lattice[0]), texel_centre(b[1], V.lattice[1]),
-                             texel_centre(b[2], V.lattice[2])};
-        const float va = functor_value(V.functor, pa[0], pa[1], pa[2]);
-        const float vb = functor_value(V.functor, pb[0], pb[1], pb[2]);
-        float ga[3], gb[3];
-        functor_gradient(V.functor, pa[0], pa[1], pa[2], ga[0], ga[1], ga[2]);
-        functor_gradient(V.functor, pb[0], pb[1], pb[2], gb[0], gb[1], gb[2]);
+        float va, vb, ga[3] = {0.f, 0.f, 0.f}, gb[3] = {0.f, 0.f, 0.f};
+        if constexpr (FT == kFieldFunctor) {
+            const float pa[3] = {texel_centre(a[0], V.lattice[0]), texel_centre(a[1], V.lattice[1]),
+                                 texel_centre(a[2], V.lattice[2])};
+            const float pb[3] = {texel_centre(b[0], V.lattice[0]), texel_centre(b[1], V.lattice[1]),
+                                 texel_centre(b[2], V.lattice[2])};
+            va = functor_value(V.functor, pa[0], pa[1], pa[2]);
+            vb = functor_value(V.functor, pb[0], pb[1], pb[2]);
+            functor_gradient(V.functor, pa[0], pa[1], pa[2], ga[0], ga[1], ga[2]);
+            functor_gradient(V.functor, pb[0], pb[1], pb[2], gb[0], gb[1], gb[2]);
+        } else if constexpr (FT == kFieldUser) {
+            const float pa[3] = {texel_centre(a[0], V.lattice[0]), texel_centre(a[1], V.lattice[1]),
+                                 texel_centre(a[2], V.lattice[2])};
+            const float pb[3] = {texel_centre(b[0], V.lattice[0]), texel_centre(b[1], V.lattice[1]),
+                                 texel_centre(b[2], V.lattice[2])};
+            va = UF::value(V.functor.p, V.functor.count, pa[0], pa[1], pa[2]);
+            vb = UF::value(V.functor.p, V.functor.count, pb[0], pb[1], pb[2]);
+            if constexpr (UF::kHasGradient) {
+                UF::gradient(V.functor.p, V.functor.count, pa[0], pa[1], pa[2], ga);
+                UF::gradient(V.functor.p, V.functor.count, pb[0], pb[1], pb[2], gb);
+            }
+        } else if constexpr (FT == kFieldF32X4) {
+            const float4 sa = fetch_rgba(V, a[0], a[1], a[2]), sb = fetch_rgba(V, b[0], b[1], b[2]);
+            va = sa.w;
+            vb = sb.w;
+            ga[0] = sa.x; ga[1] = sa.y; ga[2] = sa.z;
+            gb[0] = sb.x; gb[1] = sb.y; gb[2] = sb.z;
+        } else {
+            va = fetch<FT, UF>(V, a[0], a[1], a[2]);
+            vb = fetch<FT, UF>(V, b[0], b[1], b[2]);
+        }
         const float iso = V.iso;
         const FF tf = ff_ratio_of_diffs(va, iso, va, vb);
         t = tf.hi + tf.lo;
@@ -177,7 +204,7 @@ __device__ __forceinline__ void edge_vertex(const Volume& V, const int* a, int a
         }
     } else {
         EdgeField F;
-        gather_edge<FT, MODE == kGeomCentral>(V, a, axis, cx, cy, cz, F);
+        gather_edge<FT, MODE == kGeomCentral, UF>(V, a, axis, cx, cy, cz, F);
         const float iso = V.iso;
         t = (F.va - iso) / (F.va - F.vb);  // (f(a) - iso) / (f(a) - f(b)), relative error <= 3u
         float s2 = 0.0f, n2 = 0.0f;

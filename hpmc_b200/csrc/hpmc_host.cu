@@ -89,12 +89,14 @@ void volume_layout(Volume& V, const int lattice[3], const int cells[3], const fl
     V.nfx = (V.cells[0] + 31) / 32;
     V.nfy = (V.cells[1] + 31) / 32;
     V.column_slices = kColumnSliceChoices[3];
+    V.wait_limit_ns = kWaitLimitNs;
+    V.stall_box = -1;
     *level_entries_total = off;
     *arena_slots = V.column_layout ? (long long)V.nfx * V.nfy * V.cells[2] : V.nblocks;
 }
 
-int default_column_slices(const Volume& V, int num_sms, int ctas_per_sm) {
-    const long long target = (long long)ctas_per_sm * num_sms;
+int default_column_slices(const Volume& V, int num_sms) {
+    const long long target = (long long)kColumnsPerSm * num_sms;
     for (int zc : kColumnSliceChoices)
         if ((long long)V.nfx * V.nfy * ((V.cells[2] + zc - 1) / zc) >= target) return zc;
     return kColumnSliceChoices[3];

@@ -36,7 +36,17 @@ bool determine_layout(const int lattice[3], const int cells[3], int out[6]);
 // the driver does not provide it).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
-inline size_t elem_size(int type) { return type == HPMC_SCALAR_F32 ? 4 : 1; }
+inline size_t elem_size(int type) {
+    return type == HPMC_SCALAR_F32 ? 4 : type == HPMC_SCALAR_F32X4 ? 16 : 1;
+}
+
+// Kernel field type of an HPMCScalarType.
+inline int field_type(int scalar_type) {
+    return scalar_type == HPMC_SCALAR_F32    ? kFieldF32
+           : scalar_type == HPMC_SCALAR_U8   ? kFieldU8
+           : scalar_type == HPMC_SCALAR_F32X4 ? kFieldF32X4
+                                              : kFieldUNorm8;
+}
 
 // Geometry and compact-pyramid members of V from the lattice, the grid and
 // the layout L (everything except the field, the device pointers and iso).
@@ -44,9 +54,10 @@ inline size_t elem_size(int type) { return type == HPMC_SCALAR_F32 ? 4 : 1; }
 void volume_layout(Volume& V, const int lattice[3], const int cells[3], const float extent[3], const int L[6],
                    long long* level_entries_total, long long* arena_slots);
 
-// Slices per column CTA: the longest column that still gives about
-// `ctas_per_sm` CTAs per SM for this volume alone.
-int default_column_slices(const Volume& V, int num_sms, int ctas_per_sm);
+// Slices per column of the persistent column classifier (the single-volume
+// paths: the pyramid handle and HPMCextractStatic): the longest column that
+// still gives kColumnsPerSm columns per SM for this volume.
+int default_column_slices(const Volume& V, int num_sms);
 
 // Tensor map of the column classifier (box 36x33xkLayersPerBox f32 or
 // 48x33xkLayersPerBox uint8).  False if the driver refuses it.

@@ -19,49 +19,9 @@
 #include "hpmc_fetch.cuh"
 #include "hpmc_kernels.h"
 #include "hpmc_tma.cuh"
-#include "_gen/hpmc_case_tables.h"
+#include "hpmc_classify_core.cuh"
 
 namespace hpmc {
-
-__constant__ uint8_t c_vertex_count[256] = HPMC_GEN_VERTEX_COUNT;
-
-namespace {
-
-// The four codes of a 2x2 quad of cells from the 3-bit sample groups of its
-// three rows in the lower (gb) and upper (gt) sample layers; bit
-// (dx + 2dy + 4dz) set iff the sample is below iso (shadergen.cpp:132-153).
-__device__ __forceinline__ uint32_t quad_codes(const uint32_t gb[3], const uint32_t gt[3], bool vx0,
-                                               bool vx1, bool vy0, bool vy1) {
-    uint32_t packed = 0;
-#pragma unroll
-    for (int dy = 0; dy < 2; dy++) {
-#pragma unroll
-        for (int dx = 0; dx < 2; dx++) {
-            uint32_t c = ((gb[dy] >> dx) & 3u) | (((gb[dy + 1] >> dx) & 3u) << 2) |
-                         (((gt[dy] >> dx) & 3u) << 4) | (((gt[dy + 1] >> dx) & 3u) << 6);
-            const bool valid = (dx ? vx1 : vx0) && (dy ? vy1 : vy0);
-            if (!valid) c = 0;  // masked cells (shadergen.cpp:112-125, 163)
-            packed |= c << (8 * (dx + 2 * dy));
-        }
-    }
-    return packed;
-}
-
-__device__ __forceinline__ uint32_t quad_count(const uint8_t* s_cnt, uint32_t packed) {
-    return (uint32_t)s_cnt[packed & 0xffu] + s_cnt[(packed >> 8) & 0xffu] + s_cnt[(packed >> 16) & 0xffu] +
-           s_cnt[packed >> 24];
-}
-
-__device__ __forceinline__ void write_codes(const Volume& V, uint32_t packed, int x, int y, int z) {
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const int xx = x + (c & 1), yy = y + (c >> 1);
-        if (xx < V.cells[0] && yy < V.cells[1])
-            V.codes_out[((long long)z * V.cells[1] + yy) * V.cells[0] + xx] = (uint8_t)(packed >> (8 * c));
-    }
-}
-
-}  // namespace
 
 // ---------------------------------------------------------------------------
 // Column classification: CTA = one 32x32 cell footprint of the slice tiles,
@@ -75,8 +35,9 @@ __device__ __forceinline__ void write_codes(const Volume& V, uint32_t packed, in
 // k = bit k (dx + 2dy + 4dz) of the 32 codes.  AND/OR over the eight words
 // marks the cells that are neither all-inside nor all-outside (the only ones
 // with vertices); only those go through the count table.  The warp sum is the
-// block's level-5 entry; non-empty blocks also store their 1024 codes
-// (bit-matrix transpose) in the arena.
+// block's level-5 entry; non-empty blocks also store their active-cell list
+// (Morton order, with codes and first vertices) in the arena, so that the
+// traversal never re-reads codes or recounts a block.
 namespace {
 
 template <int FT, typename T>
@@ -112,12 +73,74 @@ __device__ __forceinline__ void slices_to_codes(const uint32_t c[8], uint32_t w[
     }
 }
 
+// 16 bits -> Morton positions of an 8x2 cell tile: bit x of the low byte goes
+// to bit (x0 | x1 << 2 | x2 << 4), bit x of the high byte to that + 8.
+__device__ __forceinline__ uint32_t spread16(uint32_t t) {
+    t = (t | (t << 12)) & 0x0F0F0F0Fu;
+    return (t | (t << 2)) & 0x33333333u;
+}
+
+// One warp: the active-cell list of a 32x32 block (lane = row y) into `list`
+// (one arena slot), from the row's 32 codes (w[i] = cells 4i..4i+3) and its
+// active-cell mask.  Lane q then owns the Morton range 32q .. 32q+31, an 8x4
+// cell tile (Morton bits x0 y0 x1 y1 x2 | y2 x3 y3 x4 y4): it gathers the
+// tile's active bits from four rows into one Morton-ordered word, reads the
+// codes of those cells from the staged rows, and one warp scan gives every
+// lane its first list slot and first vertex.  Returns the block's vertices.
+__device__ __forceinline__ uint32_t active_list_from_rows(uint32_t* list, const uint32_t w[8], uint32_t active,
+                                                          int lane, uint8_t* s_codes, const uint8_t* s_cnt) {
+    uint4* row = reinterpret_cast<uint4*>(s_codes + 32 * lane);
+    row[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    row[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    const uint32_t q = (uint32_t)lane;
+    const uint32_t y0 = 4u * ((q & 1u) | ((q >> 1) & 2u) | ((q >> 2) & 4u));
+    const uint32_t x0 = 8u * (((q >> 1) & 1u) | ((q >> 2) & 2u));
+    const uint32_t r0 = (__shfl_sync(0xffffffffu, active, (int)y0) >> x0) & 0xffu;
+    const uint32_t r1 = (__shfl_sync(0xffffffffu, active, (int)y0 + 1) >> x0) & 0xffu;
+    const uint32_t r2 = (__shfl_sync(0xffffffffu, active, (int)y0 + 2) >> x0) & 0xffu;
+    const uint32_t r3 = (__shfl_sync(0xffffffffu, active, (int)y0 + 3) >> x0) & 0xffu;
+    // rows 0/2 on Morton bit 3 = 0/1 with bit 1 = 0; rows 1/3 shifted by 2 (bit 1 = 1)
+    const uint32_t word = spread16(r0 | (r2 << 8)) | (spread16(r1 | (r3 << 8)) << 2);
+    __syncwarp();  // the staged rows are visible to the warp
+    uint32_t vsum = 0;
+    for (uint32_t m = word; m; m &= m - 1u) {
+        const uint32_t r = (uint32_t)(__ffs(m) - 1);
+        const uint32_t x = x0 + ((r & 1u) | ((r >> 1) & 2u) | ((r >> 2) & 4u));
+        const uint32_t y = y0 + (((r >> 1) & 1u) | ((r >> 2) & 2u));
+        vsum += s_cnt[s_codes[32u * y + x]];
+    }
+    // one scan of (active cells << 16 | vertices); both < 2^16 per block
+    const uint32_t mine = vsum | ((uint32_t)__popc(word) << 16);
+    uint32_t scan = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
+        if (lane >= o) scan += t;
+    }
+    const uint32_t all = __shfl_sync(0xffffffffu, scan, 31);
+    const uint32_t excl = scan - mine;
+    uint32_t vpos = excl & 0xffffu, apos = excl >> 16;
+    for (uint32_t m = word; m; m &= m - 1u) {
+        const uint32_t r = (uint32_t)(__ffs(m) - 1);
+        const uint32_t x = x0 + ((r & 1u) | ((r >> 1) & 2u) | ((r >> 2) & 4u));
+        const uint32_t y = y0 + (((r >> 1) & 1u) | ((r >> 2) & 2u));
+        const uint32_t code = s_codes[32u * y + x];
+        list[apos++] = (vpos << kListStartShift) | (code << 10) | (32u * q + r);
+        vpos += s_cnt[code];
+    }
+    list[(all >> 16) + (uint32_t)lane] = kListSentinel;
+    __syncwarp();  // the staged rows are free for the next block
+    return all & 0xffffu;
+}
+
 // One warp: classify slice z of footprint (fx, fy) from sample-bit rows of the
-// lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).
+// lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Blocks with
+// vertices get their level-5 count and their active-cell list; s_codes is the
+// warp's 1 KiB staging area.
 __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, int lane,
                                                     uint32_t vmask, const uint32_t* rows_b, uint64_t col_b,
                                                     const uint32_t* rows_t, uint64_t col_t,
-                                                    const uint8_t* s_cnt) {
+                                                    const uint8_t* s_cnt, uint8_t* s_codes) {
     // rows y and y+1 of both layers; bit 32 of a row (column x0+32) comes
     // from the column word: (row >> 1) | colbit << 31 is the row shifted by one cell
     const uint32_t cbl = (uint32_t)col_b, cbh = (uint32_t)(col_b >> 32);
@@ -139,8 +162,10 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
         all &= c[k];
         any |= c[k];
     }
-    // cells that are neither all-inside nor all-outside: the only ones with vertices
-    const bool has_vertices = __any_sync(0xffffffffu, ((all ^ any) & vmask) != 0u);
+    // cells that are neither all-inside nor all-outside: the only ones with
+    // vertices (every other MC case has at least one triangle)
+    const uint32_t active = (all ^ any) & vmask;
+    const bool has_vertices = __any_sync(0xffffffffu, active != 0u);
     const uint64_t b = column_block_index(V, z, fx, fy);
     if (!has_vertices) {
         if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = 0u;
@@ -151,38 +176,10 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
     for (int k = 0; k < 8; k++) c[k] &= vmask;
     uint32_t w[8];
     slices_to_codes(c, w);
-    uint32_t total = 0;
     if (has_vertices) {
-        uint32_t cnt = 0;
-#pragma unroll
-        for (int i = 0; i < 32; i++) cnt += s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
-        total = __reduce_add_sync(0xffffffffu, cnt);
-        if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-    }
-    if (total) {
-        // arena word for quad (qx, qy) = cells (2qx,2qy),(2qx+1,2qy),(2qx,2qy+1),(2qx+1,2qy+1):
-        // rows 2qy (even lane) and 2qy+1 (odd lane); even lanes store qx 0..7, odd 8..15
-        uint32_t p[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) p[i] = __shfl_xor_sync(0xffffffffu, w[i], 1);
-        const bool odd = lane & 1;
-        const uint32_t qy = (uint32_t)lane >> 1;
         const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
-        uint32_t* dst = V.arena + slot * kBlockWords;
-        // Morton index of quad (qx, qy), qx = (odd ? 8 : 0) + i: the bits of i
-        // (compile-time) and of the lane's part are disjoint
-        const uint32_t qys = (qy & 1u) | ((qy & 2u) << 1) | ((qy & 4u) << 2) | ((qy & 8u) << 3);
-        const uint32_t qbase = (odd ? 0x40u : 0u) | (qys << 1);
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const uint32_t wi = odd ? w[4 + (i >> 1)] : w[i >> 1];  // this lane's word with cells 2qx, 2qx+1
-            const uint32_t pi = odd ? p[4 + (i >> 1)] : p[i >> 1];
-            const uint32_t upper = odd ? wi : pi;  // row 2qy+1
-            const uint32_t lower = odd ? pi : wi;  // row 2qy
-            const uint32_t word = __byte_perm(lower, upper, (i & 1) ? 0x7632 : 0x5410);
-            const uint32_t ispread = (uint32_t)((i & 1) | ((i & 2) << 1) | ((i & 4) << 2));
-            dst[qbase | ispread] = word;
-        }
+        const uint32_t total = active_list_from_rows(V.arena + slot * kSlotWords, w, active, lane, s_codes, s_cnt);
+        if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
     }
     if (V.codes_out) {
         const int y = fy * 32 + lane;
@@ -221,8 +218,10 @@ struct ColumnSmem {
     uint64_t col[kRowBuffers];                   // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
     uint64_t bar[kRingStages];
     uint8_t cnt[256];
+    alignas(16) uint8_t codes[kWarps][32 * 32];  // per warp: the codes of the block it lists
 };
 static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4 row stores need 16-byte alignment");
+static_assert(offsetof(ColumnSmem, codes) % 16 == 0, "uint4 code stores need 16-byte alignment");
 
 // Bit rows of the nl layers of one box (stage st), layer l stored at
 // running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
@@ -261,12 +260,13 @@ __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st
 // the column's layer 0.
 __device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, int lb, int nl,
                                                     uint32_t glu, int warp, int lane, uint32_t vmask,
-                                                    const ColumnSmem& C) {
+                                                    ColumnSmem& C) {
     // the slice of this warp, if any
     const int sl = lb - 1 + (int)(((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u);
     if (sl >= 0 && sl <= lb + nl - 2) {
         const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
-        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt], C.cnt);
+        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt], C.cnt,
+                            C.codes[warp]);
     }
 }
 
@@ -310,8 +310,11 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         mbar_fence_init();
     }
     __syncthreads();
+    // test hook: the first column of the volume never receives box stall_box
+    const int stall = (fx == 0 && fy == 0 && zc == 0) ? V.stall_box : -1;
     if (tid == 0) {
         for (int k = 0; k < kRingStages && k < nbox; k++) {
+            if (k == stall) continue;
             mbar_arrive_expect_tx(&C.bar[k], G::STAGE_BYTES);
             tma_load_3d(s_ring + k * G::STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &C.bar[k]);
         }
@@ -326,14 +329,14 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         const int lb = k * kLayersPerBox;
         const int nl = min(kLayersPerBox, nlayers - lb);
         // every warp waits on the box's mbarrier (suspended in hardware, not spinning)
-        if (!mbar_wait_bounded(&C.bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout)) timed_out = true;
+        if (!mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout)) timed_out = true;
         if (!timed_out)
             convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl, (uint32_t)lb,
                             iso, u8_thr, warp, lane, C);
         // the only CTA barrier of a box: stage s consumed, bit rows of layers
         // lb .. lb+nl-1 ready, and a uniform decision on a timed-out wait
         if (__syncthreads_or(timed_out)) break;
-        if (tid == 0 && k + kRingStages < nbox) {
+        if (tid == 0 && k + kRingStages < nbox && k + kRingStages != stall) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
             tma_load_3d(s_ring + s * G::STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox,
                         &C.bar[s]);
@@ -344,8 +347,8 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         // drain the boxes still in flight (bounded) before the CTA exits
         if (tid == 0) {
             for (int l = k; l < nbox && l < k + kRingStages; l++)
-                mbar_wait_bounded(&C.bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, kWaitLimitNs, nullptr,
-                                  0u);
+                mbar_wait_bounded(&C.bar[l % kRingStages], (uint32_t)(l / kRingStages) & 1u, V.wait_limit_ns,
+                                  nullptr, 0u);
             atomicOr(&V.ctrl->status, kStatusTimeout);
         }
     }
@@ -395,8 +398,11 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         int fx, fy, z0, nl;
         column(pu, fx, fy, z0, nl);
         const int s = (int)(issued % kRingStages);
-        mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
-        tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, fx * 32, fy * 32, z0 + pk * kLayersPerBox, &C.bar[s]);
+        // test hook: CTA 0 never issues its box stall_box (its waits run out)
+        if (blockIdx.x != 0 || (int)issued != V.stall_box) {
+            mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
+            tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, fx * 32, fy * 32, z0 + pk * kLayersPerBox, &C.bar[s]);
+        }
         issued++;
         if (++pk * kLayersPerBox >= nl) {
             pk = 0;
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             const uint32_t parity = (pos / kRingStages) & 1u;
             const int lb = k * kLayersPerBox;
             const int nl = min(kLayersPerBox, nlayers - lb);
-            const bool ok = mbar_wait_bounded(&C.bar[s], parity, kWaitLimitNs, &V.ctrl->status, kStatusTimeout);
+            const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
             if (ok)
                 convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl,
                                 pos * kLayersPerBox, iso, u8_thr, warp, lane, C);
@@ -435,68 +441,11 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     if (timed_out && tid == 0) {
         // drain the boxes still in flight (bounded) before the CTA exits
         for (uint32_t p = pos; p < issued; p++)
-            mbar_wait_bounded(&C.bar[p % kRingStages], (p / kRingStages) & 1u, kWaitLimitNs, nullptr, 0u);
+            mbar_wait_bounded(&C.bar[p % kRingStages], (p / kRingStages) & 1u, V.wait_limit_ns, nullptr, 0u);
         atomicOr(&V.ctrl->status, kStatusTimeout);
     }
 }
 
-
-// ---------------------------------------------------------------------------
-// Generic classification: CTA = one 32x32 block of the virtual cell grid,
-// for any tiling (tiles narrower than 32 cells), unaligned pitches and
-// functor fields.  Each thread loads its quad's 3x3x2 samples directly.
-template <int FT>
-__device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b, uint8_t* s_cnt,
-                                                    uint32_t* s_warp) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float iso = V.binary ? 0.5f : V.iso;
-    int qx, qy;
-    morton10((uint32_t)tid, qx, qy);
-    const uint32_t X = (morton_compact(b) << 5) + 2u * (uint32_t)qx;
-    const uint32_t Y = (morton_compact(b >> 1) << 5) + 2u * (uint32_t)qy;
-    int x = 0, y = 0, z = 0;
-    uint32_t packed = 0;
-    const uint32_t tu = X >> V.wx_l2, tv = Y >> V.wy_l2;
-    if (tu < (uint32_t)V.layout_x && tv < (uint32_t)V.layout_y) {
-        x = (int)(X & ((1u << V.wx_l2) - 1u));
-        y = (int)(Y & ((1u << V.wy_l2) - 1u));
-        z = (int)((tv << V.lx_l2) | tu);
-        if (z < V.cells[2] && x < V.cells[0] && y < V.cells[1]) {
-            uint32_t gb[3], gt[3];
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                uint32_t bb = 0, bt = 0;
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    bb |= (uint32_t)(fetch<FT>(V, x + i, y + j, z) < iso) << i;
-                    bt |= (uint32_t)(fetch<FT>(V, x + i, y + j, z + 1) < iso) << i;
-                }
-                gb[j] = bb;
-                gt[j] = bt;
-            }
-            packed = quad_codes(gb, gt, true, x + 1 < V.cells[0], true, y + 1 < V.cells[1]);
-            if (V.codes_out) write_codes(V, packed, x, y, z);
-        }
-    }
-    const uint32_t cnt = __reduce_add_sync(0xffffffffu, quad_count(s_cnt, packed));
-    if (lane == 0) s_warp[warp] = cnt;
-    __syncthreads();
-    uint32_t total = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; w++) total += s_warp[w];
-    if (tid == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-    if (total) V.arena[block_slot(V, b) * kBlockWords + tid] = packed;
-    __syncthreads();
-}
-
-template <int FT>
-__global__ void __launch_bounds__(kThreads) classify_blocks(const __grid_constant__ Volume V) {
-    __shared__ uint8_t s_cnt[256];
-    __shared__ uint32_t s_warp[kWarps];
-    s_cnt[threadIdx.x] = c_vertex_count[threadIdx.x];
-    __syncthreads();
-    for (uint64_t b = blockIdx.x; b < (uint64_t)V.nblocks; b += gridDim.x) classify_block_body<FT>(V, b, s_cnt, s_warp);
-}
 
 // ---------------------------------------------------------------------------
 // Upper reductions (shadergen.cpp:174-225 without the floor filter): level
@@ -757,6 +706,7 @@ cudaError_t launch_classify(const Volume& V, const CUtensorMap* tmap, int max_ct
             case kFieldF32: classify_blocks<kFieldF32><<<grid, kThreads, 0, st>>>(V); break;
             case kFieldU8: classify_blocks<kFieldU8><<<grid, kThreads, 0, st>>>(V); break;
             case kFieldUNorm8: classify_blocks<kFieldUNorm8><<<grid, kThreads, 0, st>>>(V); break;
+            case kFieldF32X4: classify_blocks<kFieldF32X4><<<grid, kThreads, 0, st>>>(V); break;
             default: classify_blocks<kFieldFunctor><<<grid, kThreads, 0, st>>>(V); break;
         }
     }

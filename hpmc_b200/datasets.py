@@ -59,13 +59,17 @@ def noise_u8(n: int = 256, seed: int = 1, sigma: float = 3.0):
     return v.astype(np.uint8), 128.0
 
 
-def cayley(n: int = 512, seed: int = 2, noise: float = 1e-3):
+def cayley(n: int = 512, seed: int = 2, noise: float = 1e-3, slices: int | None = None):
+    """16xyz + 4(x^2+y^2+z^2) - 1 + N(0, noise) on [-1,1]^3, (z, y, x) float32.
+    `slices` keeps only the first slices (bit-identical to cayley(n)[:slices]:
+    the noise is drawn slice by slice)."""
     rng = np.random.default_rng(seed)
     xs = _grid(n, -1, 1)
-    out = np.empty((n, n, n), np.float32)
+    nz = n if slices is None else int(slices)
+    out = np.empty((nz, n, n), np.float32)
     x = xs[None, :]
     y = xs[:, None]
-    for k in range(n):
+    for k in range(nz):
         z = xs[k]
         f = 16.0 * x * y * z + 4.0 * (x * x + y * y + z * z) - 1.0
         f = f + rng.normal(0.0, noise, size=(n, n))

@@ -57,7 +57,10 @@ typedef enum HPMCStatus {
 typedef enum HPMCScalarType {
     HPMC_SCALAR_F32 = 0,     /* float */
     HPMC_SCALAR_U8 = 1,      /* uint8 read as float(b) */
-    HPMC_SCALAR_UNORM8 = 2   /* uint8 read as b/255, like a GL_ALPHA / GL_UNSIGNED_BYTE texture */
+    HPMC_SCALAR_UNORM8 = 2,  /* uint8 read as b/255, like a GL_ALPHA / GL_UNSIGNED_BYTE texture */
+    HPMC_SCALAR_F32X4 = 3    /* float4 per sample: gradient x, y, z and the value, like a GL RGBA
+                                float texture (value in alpha); the field is the value, and
+                                HPMCsetFieldTexture3D(..., GL_TRUE) uses the stored gradient */
 } HPMCScalarType;
 
 /* ---- normal estimation ---- */
@@ -97,18 +100,25 @@ void HPMCsetGridSize(struct HPMCHistoPyramid* h, GLsizei x_size, GLsizei y_size,
 void HPMCsetGridExtent(struct HPMCHistoPyramid* h, GLfloat x_extent, GLfloat y_extent, GLfloat z_extent);
 
 /* hpmc.h:404-407 / hpiface.cpp:164-184.  `texture` is a field name returned
- * by HPMCregisterDeviceField (the stand-in for a GL 3-D texture name);
- * gradient must be GL_FALSE (gradient lattices: HPMC_ERR_UNSUPPORTED). */
+ * by HPMCregisterDeviceField (the stand-in for a GL 3-D texture name).  The
+ * field is the value (alpha) channel.  gradient = GL_TRUE uses the stored
+ * gradient of an HPMC_SCALAR_F32X4 field (shadergen.cpp:260-266): t from the
+ * values at the edge ends and, as the reference computes it
+ * (shadergen.cpp:539-551), n = iso - lerp(grad a, grad b, t); with
+ * HPMC_NORMALS_CENTRAL, n = -lerp(grad a, grad b, t).  Single-channel fields
+ * read a zero gradient there, as GL's alpha textures return rgb = 0. */
 void HPMCsetFieldTexture3D(struct HPMCHistoPyramid* h, GLuint texture, GLboolean gradient);
 
-/* hpmc.h:440-444 / hpiface.cpp:187-200.  shader_source names a registered
- * device functor instead of carrying GLSL: "hpmc:cayley",
- * "hpmc:metaballs", "hpmc:twist_metaballs", "hpmc:spheres".  Any other text
- * sets HPMC_ERR_UNSUPPORTED and breaks the handle.  builder_texunit is
- * ignored.  gradient = GL_TRUE uses the functor's analytic gradient where it
- * has one (cayley): t from the functor values at the edge ends and, as the
- * reference computes it (shadergen.cpp:539-551), n = iso - lerp(grad a,
- * grad b, t); with HPMC_NORMALS_CENTRAL, n = -lerp(grad a, grad b, t). */
+/* hpmc.h:440-444 / hpiface.cpp:187-200.  shader_source names a device
+ * functor instead of carrying GLSL: a built-in one ("hpmc:cayley",
+ * "hpmc:metaballs", "hpmc:twist_metaballs", "hpmc:spheres") or one the
+ * caller registered with HPMCregisterFieldFunctor.  Any other text sets
+ * HPMC_ERR_UNSUPPORTED and breaks the handle.  builder_texunit is ignored.
+ * gradient = GL_TRUE uses the functor's analytic gradient where it has one
+ * (cayley; a registered functor with has_gradient): t from the functor
+ * values at the edge ends and, as the reference computes it
+ * (shadergen.cpp:539-551), n = iso - lerp(grad a, grad b, t); with
+ * HPMC_NORMALS_CENTRAL, n = -lerp(grad a, grad b, t). */
 void HPMCsetFieldCustom(struct HPMCHistoPyramid* h, const char* shader_source, GLuint builder_texunit,
                         GLboolean gradient);
 
@@ -174,7 +184,9 @@ GLuint HPMCregisterDeviceField(const void* device_ptr, int scalar_type, GLsizei 
 void HPMCunregisterDeviceField(GLuint name);
 
 /* Sets a device array as the field directly (lattice size from
- * HPMCsetLatticeSize).  Pitches in bytes, 0 = dense.  Taints the handle. */
+ * HPMCsetLatticeSize).  Pitches in bytes, 0 = dense.  Does not taint the
+ * handle: the field is bound at the next build (a new field therefore never
+ * disturbs work still in flight on the handle's stream). */
 int HPMCsetFieldDevice(struct HPMCHistoPyramid* h, const void* device_ptr, int scalar_type,
                        size_t row_pitch_bytes, size_t slice_pitch_bytes);
 
@@ -240,10 +252,50 @@ int HPMCsetTraversalDebugBuffers(struct HPMCTraversalHandle* th, int32_t* cell_i
  * 4 arena, 8 timeout); waits for the handle's stream. */
 int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
 
+/* Test hook for failure detection (no counterpart in the reference; it
+ * makes a bounded device wait run out without any fault).  From the next
+ * build on, the TMA column classifier's producer never issues box `box`
+ * (0-based) of its first column -- neither the expected-byte count nor the
+ * copy -- so the consumers' waits on that box give up after wait_limit_us
+ * microseconds (0: the default limit of 2 s), the CTAs drain their copies
+ * in flight and exit, and the build reports HPMC_ERR_TIMEOUT
+ * (HPMCacquireNumberOfVertices returns 0 and breaks the handle).  box < 0
+ * turns the hook off.  Builds on the generic classifier are not affected. */
+int HPMCsetTestStall(struct HPMCHistoPyramid* h, int box, unsigned int wait_limit_us);
+
 /* Classification path of the last build: 1 = TMA column kernel (every 32x32
  * cell block inside one slice tile, 16-byte aligned array field), 0 = generic
  * per-block kernel (narrow tiles, unaligned pitches, functor fields). */
 int HPMCgetClassifyPath(struct HPMCHistoPyramid* h, int* path);
+
+/* ---- caller-defined field functors ----
+ *
+ * The reference compiles whatever HPMC_fetch GLSL the application hands to
+ * HPMCsetFieldCustom into its shaders (hpmc.h:409-444).  Here the
+ * application compiles its field as a CUDA functor type in its own .cu file
+ * with include/hpmc_functor.cuh, whose HPMC_FIELD_FUNCTOR macro instantiates
+ * the classification and traversal kernels for that type in the
+ * application's device code and fills this launch table; registering the
+ * table under a name makes that name valid for HPMCsetFieldCustom.  The
+ * table is copied; the functions it points to must stay loaded while handles
+ * use the name.  Names starting with "hpmc:" are reserved. */
+#define HPMC_FIELD_FUNCTOR_ABI 1u
+typedef struct HPMCFieldFunctorOps {
+    unsigned int abi;   /* HPMC_FIELD_FUNCTOR_ABI */
+    int volume_bytes;   /* size of the volume descriptor the functor was compiled against */
+    int outputs_bytes;  /* size of the output descriptor */
+    int has_gradient;   /* the functor has an analytic gradient (HPMC_fetchGrad) */
+    /* launches the classification of the volume descriptor on a grid of `grid` CTAs */
+    int (*classify)(const void* volume, int grid, void* cuda_stream);
+    /* launches the extraction: normal_mode 0 forward, 1 central, 2 binary field */
+    int (*traverse)(const void* volume, const void* outputs, int normal_mode, int grid, void* cuda_stream);
+} HPMCFieldFunctorOps;
+
+/* No counterpart in the reference (its custom fetch is GLSL text).
+ * HPMC_ERR_INVALID_VALUE for a reserved or empty name, a NULL or mismatched
+ * table (ABI, descriptor sizes); registering a name again replaces it. */
+int HPMCregisterFieldFunctor(const char* name, const HPMCFieldFunctorOps* ops);
+int HPMCunregisterFieldFunctor(const char* name);
 
 /* ---- indexed (welded) output ----
  *
@@ -311,6 +363,11 @@ int HPMCbatchGetDeviceOffsets(struct HPMCBatch* b, const unsigned long long** de
  * traversal work item (1..64; 0 = default). */
 int HPMCbatchSetTuning(struct HPMCBatch* b, int column_slices, int traverse_ctas_per_sm, int rounds);
 int HPMCbatchGetTuning(struct HPMCBatch* b, int out[3]);
+/* Test hook (see HPMCsetTestStall): the column classifier never receives box
+ * `box` of volume `volume`'s first column; HPMCbatchGetOffsets then returns
+ * HPMC_ERR_TIMEOUT.  box < 0 turns it off (the volume index is still
+ * checked). */
+int HPMCbatchSetTestStall(struct HPMCBatch* b, int volume, int box, unsigned int wait_limit_us);
 /* Times every tuning choice on these outputs (graph replays, CUDA events)
  * and keeps the fastest; `chosen` (may be NULL) receives it. */
 int HPMCbatchAutotune(struct HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices,
@@ -332,20 +389,27 @@ int HPMCbatchAutotune(struct HPMCBatch* b, float* positions, float* normals, siz
  * The caller passes the field (device pointer, pitches in bytes, 0 = dense),
  * the outputs (float4 positions and normals, either may be NULL; capacity
  * in vertices) and a device uint32 that receives the full vertex count (so
- * that count > capacity shows truncation).  extent may be NULL (1,1,1).
- * Work is issued on `cuda_stream`.  Lattices whose pyramid and code arena do
- * not fit the scratch (e.g. larger than about 160^3) are rejected with
+ * that count > capacity shows truncation).  device_status (a device uint32,
+ * may be NULL) receives the call's device status bits, as
+ * HPMCgetDeviceStatus reports them for a handle: 1 the count does not fit
+ * 32 bits, 2 the outputs were too small (the first `capacity` vertices are
+ * written), 8 a bounded wait in the classifier gave up (HPMC_ERR_TIMEOUT:
+ * the count and the outputs of that call are invalid).  Both are written on
+ * the stream after the extraction, so no host sync is needed to read them in
+ * stream order.  extent may be NULL (1,1,1).  Work is issued on
+ * `cuda_stream`.  Lattices whose pyramid and active-cell lists do not fit
+ * the scratch (e.g. larger than about 150^3) are rejected with
  * HPMC_ERR_TOO_LARGE.  The first call on a device looks up the scratch
  * array's device address and configures the kernels, so make it before any
  * stream capture.  All calls share the one scratch array, which keeps the
  * last call's contents (the call clears what must start at zero): calls that
  * overlap on the GPU -- different streams, or concurrent host threads -- race
  * and must be serialised by the caller. */
-#define HPMC_STATIC_SCRATCH_BYTES (4u << 20)
+#define HPMC_STATIC_SCRATCH_BYTES (16u << 20)
 int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_size, GLsizei y_size, GLsizei z_size,
                       size_t row_pitch_bytes, size_t slice_pitch_bytes, GLfloat iso, int normal_mode,
                       const GLfloat* extent, float* positions, float* normals, size_t capacity_vertices,
-                      unsigned int* device_vertex_count, void* cuda_stream);
+                      unsigned int* device_vertex_count, unsigned int* device_status, void* cuda_stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -76,6 +76,9 @@ struct vec3 {
     vec2 xy() const { return vec2(x, y); }
     vec3& operator+=(const vec3& o) { x += o.x; y += o.y; z += o.z; return *this; }
     vec3& operator*=(const vec3& o) { x *= o.x; y *= o.y; z *= o.z; return *this; }
+    vec3& operator*=(float s) { x *= s; y *= s; z *= s; return *this; }
+    vec3& operator-=(float s) { x -= s; y -= s; z -= s; return *this; }
+    vec3& operator+=(float s) { x += s; y += s; z += s; return *this; }
 };
 
 struct vec4 {
@@ -113,6 +116,7 @@ inline vec3 floor(const vec3& v) { return vec3(std::floor(v.x), std::floor(v.y),
 inline vec4 floor(const vec4& v) { return vec4(std::floor(v.x), std::floor(v.y), std::floor(v.z), std::floor(v.w)); }
 inline float fract(float v) { return v - std::floor(v); }
 inline vec2 fract(const vec2& v) { return vec2(fract(v.x), fract(v.y)); }
+inline vec3 fract(const vec3& v) { return vec3(fract(v.x), fract(v.y), fract(v.z)); }
 inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float dot(const vec4& a, const vec4& b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
@@ -138,6 +142,7 @@ struct sampler2D {
 };
 struct sampler3D {
     const float* alpha = nullptr;  // x fastest, one channel (.a)
+    const float* rgba = nullptr;   // or x fastest, four channels (an RGBA float texture)
     int nx = 0, ny = 0, nz = 0;
 };
 
@@ -156,7 +161,9 @@ inline vec4 texelFetch(const sampler2D& s, const ivec2& p, int level) {
 }
 inline vec4 texture3D(const sampler3D& s, const vec3& p) {
     const int i = nearest(p.x, s.nx), j = nearest(p.y, s.ny), k = nearest(p.z, s.nz);
-    return vec4(0.f, 0.f, 0.f, s.alpha[((size_t)k * s.ny + j) * s.nx + i]);
+    const size_t o = ((size_t)k * s.ny + j) * s.nx + i;
+    if (s.rgba) return vec4(s.rgba[4 * o], s.rgba[4 * o + 1], s.rgba[4 * o + 2], s.rgba[4 * o + 3]);
+    return vec4(0.f, 0.f, 0.f, s.alpha[o]);  // a GL_ALPHA texture reads rgb = 0
 }
 
 }  // namespace glsl

@@ -8,8 +8,12 @@ see oracle/Makefile) -- rewrites the few constructs C++ does not share with
 GLSL (uniform declarations, float literals, swizzles, `out` parameters, the
 name `main`), compiles it against oracle/glsl_emu.hpp with the host compiler,
 and drives the passes the way buildpass.cpp:42-178 and triface.cpp:332-457 do
-(texture-field mode, GL 3 targets): base level, first reduction (floor
-filter), upper reductions, then extractVertex for every vertex id.
+(GL 3 targets): base level, first reduction (floor filter), upper reductions,
+then extractVertex for every vertex id.  Field modes: a Texture3D field
+(alpha texture, or an RGBA float texture whose .xyz the gradient mode reads),
+or the custom-fetch mode with an application's GLSL snippet
+(HPMCsetFieldCustom); binary fields bind the edge table with table normals
+(triface.cpp:391-399).
 
 The outputs (every mip level, the vertex count, positions and normals in
 FP32 GLSL arithmetic) pin the oracle's restatement to the reference's code.
@@ -53,7 +57,7 @@ def translate(text: str) -> str:
 
 _DRIVER = r"""
 #include <omp.h>
-extern "C" int glsl_run(const float* field, int fx, int fy, int fz, float iso, int size, int size_l2,
+extern "C" int glsl_run(const float* field, int rgba, int fx, int fy, int fz, float iso, int size, int size_l2,
                         const float* count_rgba, const float* edge_rgba, float* mips, int max_vertices,
                         float* pos, float* nrm, int threads) {
     if (threads > 0) omp_set_num_threads(threads);
@@ -61,7 +65,8 @@ extern "C" int glsl_run(const float* field, int fx, int fy, int fz, float iso, i
     std::vector<std::vector<float>> mip(size_l2 + 1);
     mip[0].assign((size_t)size * size * 4, 0.f);
     sampler3D field_tex;
-    field_tex.alpha = field; field_tex.nx = fx; field_tex.ny = fy; field_tex.nz = fz;
+    if (rgba) field_tex.rgba = field; else field_tex.alpha = field;
+    field_tex.nx = fx; field_tex.ny = fy; field_tex.nz = fz;
     sampler1D count_tex;
     count_tex.rgba = count_rgba; count_tex.n = 256;
 #pragma omp parallel
@@ -140,9 +145,12 @@ extern "C" int glsl_run(const float* field, int fx, int fy, int fz, float iso, i
 """
 
 
-def program(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
-    """C++ source of the reference's passes for one configuration."""
-    g = lambda which: O.ref_glsl(which, lattice, cells, extent)  # noqa: E731
+def program(lattice, cells=None, extent=(1.0, 1.0, 1.0), binary=False, gradient=False,
+            custom: str | None = None) -> str:
+    """C++ source of the reference's passes for one configuration (custom:
+    the application's GLSL fetch snippet of the custom-fetch mode)."""
+    g = lambda which: O.ref_glsl(which, lattice, cells, extent, binary=binary, gradient=gradient,  # noqa: E731
+                                 custom_source=custom)
     defines, fetch = g(0), translate(g(1))
     parts = ['#include "glsl_emu.hpp"', "#include <algorithm>", "using namespace glsl;", translate(defines)]
     # uniforms and built-ins are per-thread: the harness runs fragments and
@@ -161,9 +169,10 @@ def program(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
     return "\n".join(parts)
 
 
-def build(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
+def build(lattice, cells=None, extent=(1.0, 1.0, 1.0), binary=False, gradient=False,
+          custom: str | None = None) -> str:
     """Compile the passes of one configuration into a shared library (cached)."""
-    src = program(lattice, cells, extent)
+    src = program(lattice, cells, extent, binary, gradient, custom)
     key = hashlib.sha1((src + open(os.path.join(HERE, "glsl_emu.hpp")).read()).encode()).hexdigest()[:16]
     os.makedirs(OUT, exist_ok=True)
     so = os.path.join(OUT, f"glsl_{key}.so")
@@ -180,31 +189,37 @@ def build(lattice, cells=None, extent=(1.0, 1.0, 1.0)) -> str:
     return so
 
 
-def run(field: np.ndarray, iso: float, cells=None, extent=(1.0, 1.0, 1.0), max_vertices: int = 1 << 20,
-        threads: int = 0, keep_levels: bool = True):
-    """The reference's passes on a float field (z, y, x) as a float alpha
-    texture, on `threads` host threads (0: all).  Returns (mip levels as
-    (w, w, 4) arrays -- empty unless keep_levels --, vertex count, positions
-    (n, 3), normals (n, 3)), all FP32 as the shaders compute them."""
-    fz, fy, fx = field.shape
+def run(field: np.ndarray | None, iso: float, cells=None, extent=(1.0, 1.0, 1.0), max_vertices: int = 1 << 20,
+        threads: int = 0, keep_levels: bool = True, *, binary=False, gradient=False, custom: str | None = None,
+        shape=None):
+    """The reference's passes on `threads` host threads (0: all).  `field`:
+    a float (z, y, x) array bound as an alpha texture, a (z, y, x, 4) array
+    bound as an RGBA float texture (gradient = True reads its .xyz), or None
+    with `custom` (the custom-fetch snippet) and `shape` = (z, y, x).
+    Returns (mip levels as (w, w, 4) arrays -- empty unless keep_levels --,
+    vertex count, positions (n, 3), normals (n, 3)), all FP32 as the shaders
+    compute them."""
+    fz, fy, fx = (shape if field is None else field.shape[:3])
     lattice = (fx, fy, fz)
     L = O.layout(lattice, cells)
-    lib = C.CDLL(build(lattice, cells, extent))
-    count, _, ed, _ = O.tables()
+    lib = C.CDLL(build(lattice, cells, extent, binary, gradient, custom))
+    count, _, ed, edn = O.tables()
     count_rgba = np.zeros((256, 4), np.float32)
     count_rgba[:, 3] = count
-    edge_rgba = np.ascontiguousarray(ed.reshape(256, 16, 4).astype(np.float32))
+    # binary fields: the table with normals in the fractions (triface.cpp:391-399)
+    edge_rgba = np.ascontiguousarray((edn if binary else ed).reshape(256, 16, 4).astype(np.float32))
     size, l2 = L.size, L.size_l2
     mips_len = sum((size >> m) ** 2 * 4 for m in range(l2 + 1))
     mips = np.zeros(mips_len if keep_levels else 1, np.float32)
     pos = np.zeros((max_vertices, 3), np.float32)
     nrm = np.zeros((max_vertices, 3), np.float32)
-    f = np.ascontiguousarray(field, dtype=np.float32)
+    f = np.zeros(4, np.float32) if field is None else np.ascontiguousarray(field, dtype=np.float32)
+    rgba = int(field is not None and field.ndim == 4)
     fn = lib.glsl_run
     fn.restype = C.c_int
     p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
     threads = int(threads) if threads and threads > 0 else (os.cpu_count() or 1)
-    n = fn(p(f), fx, fy, fz, C.c_float(iso), size, l2, p(count_rgba), p(edge_rgba),
+    n = fn(p(f), rgba, fx, fy, fz, C.c_float(iso), size, l2, p(count_rgba), p(edge_rgba),
            p(mips) if keep_levels else None, max_vertices, p(pos), p(nrm), threads)
     levels, off = [], 0
     for m in range(l2 + 1 if keep_levels else 0):

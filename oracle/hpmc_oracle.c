@@ -206,6 +206,13 @@ static float functor_value(const oracle_functor_t* F, float px, float py, float 
         }
         return d;
     }
+    case 5: {
+        /* a caller-registered functor (hpmc_b200/apps/custom_functor.cu): the
+         * torus (sqrt(x^2 + y^2) - R)^2 + z^2 - r^2 on [-1,1]^3, p = {R, r} */
+        const float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        const float d = sqrtf(x * x + y * y) - F->p[0];
+        return d * d + z * z - F->p[1] * F->p[1];
+    }
     default:
         return 0.0f;
     }
@@ -219,6 +226,13 @@ static void functor_gradient(const oracle_functor_t* F, float px, float py, floa
         g[0] = -16.0f * y * z - 8.0f * x;
         g[1] = -16.0f * x * z - 8.0f * y;
         g[2] = -16.0f * x * y - 8.0f * z;
+    } else if (F->id == 5) {
+        const float x = 2.0f * px - 1.0f, y = 2.0f * py - 1.0f, z = 2.0f * pz - 1.0f;
+        const float q = sqrtf(x * x + y * y);
+        const float d = q - F->p[0];
+        g[0] = 2.0f * d * x / q;
+        g[1] = 2.0f * d * y / q;
+        g[2] = 2.0f * z;
     } else {
         g[0] = g[1] = g[2] = 0.0f;
     }
@@ -240,6 +254,7 @@ static inline float sample_f(const void* field, int type, const oracle_layout_t*
     z = clampl(z, 0, L->lattice[2] - 1);
     size_t off = (size_t)z * sp + (size_t)y * rp + (size_t)x;
     if (type == ORACLE_F32) return ((const float*)field)[off];
+    if (type == ORACLE_F32X4) return ((const float*)field)[4 * off + 3]; /* texture3D(...).a */
     uint8_t b = ((const uint8_t*)field)[off];
     if (type == ORACLE_U8) return (float)b;
     return (float)b / 255.0f;
@@ -464,6 +479,31 @@ void oracle_geometry(const void* field, int type, const oracle_layout_t* L, size
             for (int i = 0; i < 3; i++) {
                 float fr = en[i] - floorf(en[i]);
                 nn[i] = 2.0 * (double)fr - 1.0;
+            }
+        } else if (normal_mode >= ORACLE_NORMALS_GRADIENT && type != ORACLE_FUNCTOR) {
+            /* HPMC_sampleGrad of a texture (shadergen.cpp:260-266): the RGBA
+             * sample at each edge end, value in .a, gradient in .rgb (zero for
+             * a single-channel field) */
+            double va = oracle_sample(field, type, L, rp, sp, a[0], a[1], a[2]);
+            double vb = oracle_sample(field, type, L, rp, sp, b[0], b[1], b[2]);
+            double ga[3] = {0.0, 0.0, 0.0}, gb[3] = {0.0, 0.0, 0.0};
+            if (type == ORACLE_F32X4) {
+                const float* f4 = (const float*)field;
+                const size_t oa = 4 * ((size_t)clampl(a[2], 0, L->lattice[2] - 1) * sp +
+                                       (size_t)clampl(a[1], 0, L->lattice[1] - 1) * rp +
+                                       (size_t)clampl(a[0], 0, L->lattice[0] - 1));
+                const size_t ob = 4 * ((size_t)clampl(b[2], 0, L->lattice[2] - 1) * sp +
+                                       (size_t)clampl(b[1], 0, L->lattice[1] - 1) * rp +
+                                       (size_t)clampl(b[0], 0, L->lattice[0] - 1));
+                for (int i = 0; i < 3; i++) {
+                    ga[i] = f4[oa + i];
+                    gb[i] = f4[ob + i];
+                }
+            }
+            t = (va - thr) / (va - vb);
+            for (int i = 0; i < 3; i++) {
+                const double g = (1.0 - t) * ga[i] + t * gb[i];
+                nn[i] = normal_mode == ORACLE_NORMALS_GRADIENT ? thr - g : -g;
             }
         } else if (normal_mode >= ORACLE_NORMALS_GRADIENT && type == ORACLE_FUNCTOR) {
             const oracle_functor_t* F = (const oracle_functor_t*)field;

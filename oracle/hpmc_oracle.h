@@ -28,23 +28,28 @@ extern "C" {
 #endif
 
 enum { ORACLE_F32 = 0, ORACLE_U8 = 1, ORACLE_UNORM8 = 2, ORACLE_F64 = 3 /* geometry and adjoint only */,
-       ORACLE_FUNCTOR = 4 /* `field` points to an oracle_functor_t */ };
+       ORACLE_FUNCTOR = 4 /* `field` points to an oracle_functor_t */,
+       ORACLE_F32X4 = 5 /* float4 samples (gradient x, y, z, value): a GL RGBA float texture whose
+                           alpha is the field (shadergen.cpp:260-266); pitches in float4s */ };
 
 /* A field functor: the custom fetch snippet of HPMCsetFieldCustom
  * (hpiface.cpp:187-200, shadergen.cpp:270-286) evaluated at normalised texel
  * centres ((i + 0.5) / n per axis, no clamping).  Ids: 1 cayley
  * (apps/cayley/cayley.cpp:75-94), 2 metaballs {n, (cx,cy,cz,r) x n},
  * 3 twisted metaballs {twist, (cx,cy,cz) x 8} (apps/metaballs/metaballs.cpp:
- * 72-94), 4 union of spheres (signed distance) {n, (cx,cy,cz,r) x n}. */
+ * 72-94), 4 union of spheres (signed distance) {n, (cx,cy,cz,r) x n},
+ * 5 torus {R, r}, with gradient (the caller-registered functor of the
+ * custom-functor example app). */
 typedef struct oracle_functor_t {
     int id;
     int count;
     float p[136];
 } oracle_functor_t;
-/* Normals.  The GRADIENT modes use a functor's analytic gradient
- * (HPMC_fetchGrad, shadergen.cpp:539-551): t from the functor values at the
- * edge ends; n = iso - lerp(grad a, grad b, t) (the reference) or
- * -lerp(grad a, grad b, t). */
+/* Normals.  The GRADIENT modes use HPMC_fetchGrad (shadergen.cpp:260-266,
+ * 539-551): a functor's analytic gradient, the .xyz of an ORACLE_F32X4
+ * field, or zero for a single-channel field (a GL alpha texture reads
+ * rgb = 0); t from the values at the edge ends; n = iso - lerp(grad a,
+ * grad b, t) (the reference) or -lerp(grad a, grad b, t). */
 enum { ORACLE_NORMALS_FORWARD = 0, ORACLE_NORMALS_CENTRAL = 1, ORACLE_NORMALS_GRADIENT = 2,
        ORACLE_NORMALS_GRADIENT_CENTRAL = 3 };
 

@@ -18,7 +18,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REF_DIR = os.path.join(_HERE, "_ref")
 
-F32, U8, UNORM8, F64, FUNCTOR = 0, 1, 2, 3, 4  # F64: geometry and adjoint only
+F32, U8, UNORM8, F64, FUNCTOR, F32X4 = 0, 1, 2, 3, 4, 5  # F64: geometry and adjoint only
+# F32X4: (z, y, x, 4) float32 = gradient x, y, z and the value (a GL RGBA texture)
 NORMALS_FORWARD, NORMALS_CENTRAL = 0, 1
 # analytic-gradient normals of a functor field: the reference's iso - lerp(grad), or -lerp(grad)
 NORMALS_GRADIENT, NORMALS_GRADIENT_CENTRAL = 2, 3
@@ -117,6 +118,9 @@ def ref():
         R.hpmc_ref_midpoint_table.restype = C.POINTER(C.c_float)
         R.hpmc_ref_glsl.argtypes = [C.c_int, ip, ip, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
         R.hpmc_ref_glsl.restype = C.c_void_p
+        R.hpmc_ref_glsl_custom.argtypes = [C.c_int, ip, ip, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int,
+                                           C.c_char_p]
+        R.hpmc_ref_glsl_custom.restype = C.c_void_p
         R.hpmc_ref_free.argtypes = [C.c_void_p]
         _ref = R
     return _ref
@@ -134,7 +138,8 @@ class Functor:
     """A field functor on a lattice of `shape` (z, y, x): the oracle's form of
     HPMCsetFieldCustom + HPMCsetBuilderUniforms (hpiface.cpp:187-222)."""
 
-    IDS = {"hpmc:cayley": 1, "hpmc:metaballs": 2, "hpmc:twist_metaballs": 3, "hpmc:spheres": 4}
+    IDS = {"hpmc:cayley": 1, "hpmc:metaballs": 2, "hpmc:twist_metaballs": 3, "hpmc:spheres": 4,
+           "app:torus": 5}  # app:torus: the caller-registered functor of hpmc_b200/apps/custom_functor.cu
 
     def __init__(self, name: str, params, shape):
         self.name = name
@@ -196,13 +201,18 @@ def ref_tables():
 
 
 def ref_glsl(which: int, lattice, cells=None, extent=(1.0, 1.0, 1.0), binary=False,
-             gradient=False, gl_target=9) -> str:
+             gradient=False, gl_target=9, custom_source: str | None = None) -> str:
     """GLSL text the reference generates (which: 0 defines, 1 fetch, 2 base
-    level, 3 first reduction, 4 upper reduction, 5 extract vertex)."""
+    level, 3 first reduction, 4 upper reduction, 5 extract vertex); with
+    custom_source, for the custom-fetch mode with that application snippet."""
     lattice = [int(v) for v in lattice]
     cells = [v - 1 for v in lattice] if cells is None else [int(v) for v in cells]
-    p = ref().hpmc_ref_glsl(which, (C.c_int * 3)(*lattice), (C.c_int * 3)(*cells),
-                            (C.c_float * 3)(*extent), int(binary), int(gradient), int(gl_target))
+    args = (which, (C.c_int * 3)(*lattice), (C.c_int * 3)(*cells), (C.c_float * 3)(*extent), int(binary),
+            int(gradient), int(gl_target))
+    if custom_source is None:
+        p = ref().hpmc_ref_glsl(*args)
+    else:
+        p = ref().hpmc_ref_glsl_custom(*args, custom_source.encode())
     if not p:
         raise ValueError("layout rejected")
     s = C.string_at(p).decode()
@@ -220,6 +230,8 @@ def tables():
 
 
 def _field_type(field: np.ndarray, unorm: bool) -> int:
+    if field.dtype == np.float32 and field.ndim == 4 and field.shape[3] == 4:
+        return F32X4
     if field.dtype == np.float32:
         return F32
     if field.dtype == np.float64:

@@ -129,6 +129,31 @@ char* hpmc_ref_glsl(int which, const int lattice[3], const int cells[3],
     return strdup(src.c_str());
 }
 
+/* The same for the custom-fetch mode (HPMCsetFieldCustom, hpiface.cpp:187-200):
+ * `source` is the application's GLSL snippet defining HPMC_fetch (and, with
+ * gradient, HPMC_fetchGrad), spliced in by HPMCgenerateScalarFieldFetch
+ * (shadergen.cpp:270-286). */
+char* hpmc_ref_glsl_custom(int which, const int lattice[3], const int cells[3], const float extent[3],
+                           int binary, int gradient, int gl_target, const char* source)
+{
+    RefState s;
+    init_state(s, lattice, cells, extent, binary, gradient, gl_target);
+    s.h.m_fetch.m_mode = HPMC_VOLUME_LAYOUT_CUSTOM;
+    s.h.m_fetch.m_shader_source = source ? source : "";
+    if (!HPMCdetermineLayout(&s.h)) return nullptr;
+    std::string src;
+    switch (which) {
+        case 0: src = HPMCgenerateDefines(&s.h); break;
+        case 1: src = HPMCgenerateScalarFieldFetch(&s.h); break;
+        case 2: src = HPMCgenerateBaselevelShader(&s.h); break;
+        case 3: src = HPMCgenerateReductionShader(&s.h, "floor"); break;
+        case 4: src = HPMCgenerateReductionShader(&s.h, ""); break;
+        case 5: src = HPMCgenerateExtractVertexFunction(&s.h); break;
+        default: return nullptr;
+    }
+    return strdup(src.c_str());
+}
+
 void hpmc_ref_free(char* p) { free(p); }
 
 }  // extern "C"

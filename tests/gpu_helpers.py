@@ -8,13 +8,16 @@ EPS32 = np.finfo(np.float32).eps
 
 
 def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=False, unorm=False,
-            normals=0, capture_codes=True, pitch_pad=0, tensor=None, gradient=False):
+            normals=0, capture_codes=True, pitch_pad=0, tensor=None, gradient=False, texture=False):
     """Build + count + extract through the C ABI.  Returns a dict of numpy arrays.
-    `field` is a numpy array or an oracle Functor (registered device functor)."""
+    `field` is a numpy array ((z, y, x), or (z, y, x, 4) float32 gradient +
+    value) or an oracle Functor (registered device functor).  texture=True
+    (implied by gradient on an array) binds the array the reference's way:
+    HPMCregisterDeviceField + HPMCsetFieldTexture3D(name, gradient)."""
     import torch
 
     dev = torch.device("cuda:0")
-    fz, fy, fx = field.shape
+    fz, fy, fx = field.shape[:3]
     functor = hasattr(field, "params")
     if functor:
         pass
@@ -28,12 +31,17 @@ def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=Fals
     c = hpmc.default_constants()
     hp = hpmc.HistoPyramid(c)
     hp.set_stream(torch.cuda.current_stream())
+    name = None
     if functor:
         hp.set_lattice_size(fx, fy, fz)
         hp.set_field_custom(field.name, gradient=gradient)
         assert hp.builder_program() != 0
         if field.params:
             hp.set_builder_uniforms(field.params)
+    elif texture or gradient:
+        hp.set_lattice_size(fx, fy, fz)
+        name = hpmc.register_device_field(tensor, unorm=unorm)
+        hp.set_field_texture3d(name, gradient=gradient)
     else:
         hp.set_field_device(tensor, unorm=unorm)
     if cells is not None:
@@ -73,11 +81,13 @@ def run_gpu(hpmc, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=Fals
         out["codes"] = codes_t.cpu().numpy()
     th.close()
     hp.close()
+    if name is not None:
+        hpmc.unregister_device_field(name)
     return out
 
 
 def oracle_expect(O, field, iso, *, cells=None, extent=(1.0, 1.0, 1.0), binary=False, unorm=False, normals=0):
-    fz, fy, fx = field.shape
+    fz, fy, fx = field.shape[:3]
     L = O.layout((fx, fy, fz), cells)
     codes = O.codes(field, L, iso, binary=binary, unorm=unorm)
     levels, total = O.pyramid(codes, L)

@@ -24,7 +24,8 @@ def test_apps_built(apps):
 
 
 @pytest.mark.parametrize("name,args", [("texture3d", ["64", "64"]), ("cayley", ["1", "2"]),
-                                       ("metaballs", ["1", "2"]), ("transform_feedback", ["1", "2"])])
+                                       ("metaballs", ["1", "2"]), ("transform_feedback", ["1", "2"]),
+                                       ("custom_functor", ["1", "2"])])
 def test_apps_reject_bad_arguments(apps, name, args):
     r = subprocess.run([apps[name], *args], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "Usage" in r.stderr
@@ -114,3 +115,29 @@ def test_transform_feedback_app(apps, oracle, hpmc, tmp_path):
     p, q = _read_ply(ply)
     np.testing.assert_allclose(p, g["pos"][:, :3], rtol=0, atol=1e-6)
     np.testing.assert_allclose(q, g["nrm"][:, :3], rtol=0, atol=1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags,normals", [([], 0), (["--central"], 1), (["--gradient"], 2),
+                                           (["--gradient", "--central"], 3)])
+def test_custom_functor_app_matches_oracle(apps, oracle, tmp_path, flags, normals):
+    """A caller's own functor type (hpmc_b200/apps/custom_functor.cu: a torus,
+    compiled with include/hpmc_functor.cuh into the app's device code and
+    registered as "app:torus") against the oracle's restatement of the same
+    functor: the vertex count exactly, every vertex in order within the
+    parity tolerances (positions 1e-5 of the spacing + 4 ulp, normals 1e-5 rad)."""
+    from tests.gpu_helpers import angle, oracle_expect
+
+    shape = (56, 40, 48)  # (z, y, x)
+    ply = tmp_path / "torus.ply"
+    n = _run(apps["custom_functor"], ["48", "40", "56", "--iso", "0", "--frames", "2", "--ply", str(ply), *flags])
+    F = oracle.Functor("app:torus", [0.5, 0.25], shape)
+    e = oracle_expect(oracle, F, 0.0, normals=normals)
+    assert n == e["total"] > 0
+    p, q = _read_ply(ply)
+    spacing = 1.0 / np.array(e["L"].cells, np.float64)
+    dp = np.abs(p.astype(np.float64) - e["pos"])
+    assert (dp <= 1e-5 * spacing + 4 * np.finfo(np.float32).eps * np.abs(e["pos"])).all()
+    ang, _, nb = angle(q, e["nrm"])
+    ok = nb > 1e-6 * nb.max()
+    assert ang[ok].max() <= 1e-5

@@ -68,6 +68,31 @@ def test_null_handle_conventions(hpmc):
     L.HPMCunregisterDeviceField(name)
 
 
+class _FunctorOps(C.Structure):
+    """HPMCFieldFunctorOps (include/hpmc.h)."""
+
+    _fields_ = [("abi", C.c_uint), ("volume_bytes", C.c_int), ("outputs_bytes", C.c_int),
+                ("has_gradient", C.c_int), ("classify", C.c_void_p), ("traverse", C.c_void_p)]
+
+
+def test_functor_registration_rules(hpmc):
+    """HPMCregisterFieldFunctor checks the table before it keeps it: reserved
+    and empty names, NULL tables, a wrong ABI version, descriptor sizes or
+    missing launchers are refused (no CUDA call is made)."""
+    from hpmc_b200 import _capi
+
+    L = hpmc.lib()
+    dummy = C.cast(C.pointer(C.c_int(0)), C.c_void_p)  # never called: only checked for NULL
+    bad = [_FunctorOps(1, 0, 0, 0, dummy, dummy), _FunctorOps(99, 1, 1, 0, dummy, dummy),
+           _FunctorOps(1, 1, 1, 0, None, dummy)]
+    for ops in bad:
+        assert L.HPMCregisterFieldFunctor(b"app:x", C.byref(ops)) == _capi.ERR_INVALID_VALUE
+    assert L.HPMCregisterFieldFunctor(b"app:x", None) == _capi.ERR_INVALID_VALUE
+    assert L.HPMCregisterFieldFunctor(b"hpmc:cayley", None) == _capi.ERR_INVALID_VALUE
+    assert L.HPMCregisterFieldFunctor(b"", None) == _capi.ERR_INVALID_VALUE
+    assert L.HPMCunregisterFieldFunctor(b"app:never-registered") == _capi.ERR_INVALID_VALUE
+
+
 def test_no_cpu_fallback_without_library(monkeypatch, tmp_path):
     """The product raises when its CUDA library is missing."""
     import hpmc_b200._capi as capi

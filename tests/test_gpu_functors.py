@@ -77,3 +77,32 @@ def test_twisted_metaballs_close_to_oracle(hpmc, oracle):
     assert e["total"] > 1000
     assert abs(g["n"] - e["total"]) <= 0.01 * e["total"]
     assert np.count_nonzero(g["codes"] != e["codes"]) <= 0.001 * g["codes"].size
+
+
+@pytest.mark.parametrize("shape", [(21, 34, 30), (40, 48, 64)])
+@pytest.mark.parametrize("normals", [0, 1, 2, 3])
+def test_rgba_gradient_textures_match_oracle(hpmc, oracle, shape, normals):
+    """HPMCsetFieldTexture3D on an RGBA float texture (HPMC_SCALAR_F32X4:
+    gradient in .xyz, the field in .w).  Modes 0/1: forward/central
+    differences of the value channel; 2/3: the stored gradient
+    (shadergen.cpp:260-266, 539-551), n = iso - lerp(grad) or -lerp(grad)."""
+    rng = np.random.default_rng(sum(shape) + normals)
+    field = rng.normal(size=shape + (4,)).astype(np.float32)
+    field[..., 3][rng.random(shape) < 0.05] = 0.5  # ties with iso
+    iso = 0.5
+    gradient = normals >= 2
+    g = run_gpu(hpmc, field, iso, normals=normals % 2, gradient=gradient, texture=True)
+    e = oracle_expect(oracle, field, iso, normals=normals)
+    assert g["path"] == 0  # float4 fields take the generic classifier
+    compare(g, e)
+
+
+def test_gradient_mode_on_a_scalar_texture_reads_zero_gradient(hpmc, oracle):
+    """A single-channel texture in gradient mode: GL's alpha texture reads
+    rgb = 0, so the reference's normal is iso - 0 = iso (scaled); the oracle
+    restates that."""
+    rng = np.random.default_rng(8)
+    field = rng.normal(size=(20, 22, 24)).astype(np.float32)
+    g = run_gpu(hpmc, field, 0.25, gradient=True, texture=True)
+    e = oracle_expect(oracle, field, 0.25, normals=oracle.NORMALS_GRADIENT)
+    compare(g, e)

@@ -243,6 +243,52 @@ def test_caller_kernels_on_the_stream_stay_ordered(hpmc, oracle):
     hp.close()
 
 
+def test_retaint_between_extractions_stays_stream_ordered(hpmc, oracle):
+    """A setter that taints the handle (here the grid extent) between an
+    asynchronous extraction and the next build must not disturb the
+    extraction still in flight: the lazy set-up clears the pyramid and the
+    control block in stream order.  No host sync between the two volumes,
+    on a non-blocking stream."""
+    import torch
+
+    from hpmc_b200 import datasets
+
+    dev = torch.device("cuda:0")
+    fa, iso = datasets.cayley(256)
+    fb = np.ascontiguousarray(fa[::-1, :, :] * np.float32(1.25) - np.float32(0.02))
+    ext_b = (2.0, 1.5, 0.75)
+    ea = oracle_expect(oracle, fa, iso, normals=1)
+    eb = oracle_expect(oracle, fb, iso, normals=1, extent=ext_b)
+    ta, tb = torch.from_numpy(fa).to(dev), torch.from_numpy(fb).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    hp = hpmc.HistoPyramid(hpmc.default_constants())
+    hp.set_stream(stream)
+    hp.set_normal_mode(1)
+    hp.set_field_device(ta)
+    th = hpmc.TraversalHandle(hp)
+    pa = torch.full((ea["total"], 4), float("nan"), dtype=torch.float32, device=dev)
+    na = torch.full_like(pa, float("nan"))
+    pb = torch.full((eb["total"], 4), float("nan"), dtype=torch.float32, device=dev)
+    nb = torch.full_like(pb, float("nan"))
+    torch.cuda.synchronize()
+    for _ in range(3):
+        hp.set_field_device(ta)
+        hp.set_grid_extent(1.0, 1.0, 1.0)  # taints: set-up runs at the next build
+        hp.build(iso)
+        th.extract_to(pa, na, ea["total"], sync=False)
+        hp.set_grid_extent(*ext_b)  # taints again while A's extraction is in flight
+        hp.set_field_device(tb)
+        hp.build(iso)
+        th.extract_to(pb, nb, eb["total"], sync=False)
+    stream.synchronize()
+    for pos, e, ext in ((pa, ea, (1.0, 1.0, 1.0)), (pb, eb, ext_b)):
+        spacing = np.array(ext) / np.array(e["L"].cells, np.float64)
+        dp = np.abs(pos[:, :3].cpu().numpy().astype(np.float64) - e["pos"])
+        assert (dp <= 1e-5 * spacing[None, :] + 4 * np.finfo(np.float32).eps * np.abs(e["pos"])).all()
+    th.close()
+    hp.close()
+
+
 def test_binary_mode_and_feedback_capture(hpmc, oracle):
     """Binary fields (midpoints + table normals) and the N3F_V3F capture."""
     import torch

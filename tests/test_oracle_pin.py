@@ -116,6 +116,17 @@ def test_product_table_generator_matches_oracle(oracle):
     assert np.array_equal((np.float32(2) * fr - np.float32(1)).astype(np.float32), bn[:, :15])
 
 
+def test_every_mixed_case_has_vertices(oracle):
+    """The classifier lists a cell as active iff its 8 corners are neither all
+    inside nor all outside, without a table lookup.  That is exact only if the
+    reference's count table gives every such case at least one triangle (a
+    listed cell with no vertices would shift the traversal's cell mapping)."""
+    cnt, _, _, _ = oracle.tables()
+    cnt = np.asarray(cnt).reshape(256)
+    assert cnt[0] == 0 and cnt[255] == 0
+    assert (cnt[1:255] >= 3).all() and (cnt % 3 == 0).all() and cnt.max() <= 15
+
+
 def _brute_codes(field, iso, cells):
     cx, cy, cz = cells
     f = field.astype(np.float64) if field.dtype != np.uint8 else field.astype(np.float32)
