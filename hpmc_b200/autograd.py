@@ -21,10 +21,32 @@ import torch
 from . import (NORMALS_FORWARD, HistoPyramid, TraversalHandle, default_constants)
 
 
+# Pyramid + traversal handles reused across calls, per (device, field shape,
+# dtype, strides): a forward borrows a pair and gives it back right away when
+# no gradient will be asked for, otherwise after its backward.  No device
+# allocation per call once the pool holds a pair for the shape.
+_POOL: dict = {}
+
+
+def _borrow(field):
+    key = (str(field.device), tuple(field.shape), field.dtype, tuple(field.stride()))
+    free = _POOL.setdefault(key, [])
+    if free:
+        return key, free.pop()
+    hp = HistoPyramid(default_constants())
+    hp.set_field_device(field)  # sizes the pyramid once for this shape
+    return key, (hp, TraversalHandle(hp))
+
+
+def _give_back(key, handles):
+    handles[0]._keep.clear()  # the pool does not keep the caller's field alive
+    _POOL.setdefault(key, []).append(handles)
+
+
 class ExtractFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, field, iso, normals, extent):
-        hp = HistoPyramid(default_constants())
+        key, (hp, th) = _borrow(field)
         hp.set_stream(torch.cuda.current_stream())
         hp.set_field_device(field)
         hp.set_grid_extent(*extent)
@@ -34,31 +56,36 @@ class ExtractFunction(torch.autograd.Function):
         if hp.last_error:
             from . import HPMCError
 
-            raise HPMCError(hp.last_error, "HPMCbuildHistopyramid")
-        th = TraversalHandle(hp)
+            err = hp.last_error
+            _give_back(key, (hp, th))
+            raise HPMCError(err, "HPMCbuildHistopyramid")
         pos = torch.empty((n, 4), dtype=torch.float32, device=field.device)
         nrm = torch.empty((n, 4), dtype=torch.float32, device=field.device)
         if n:
             th.extract_to(pos, nrm, n, sync=False)
-        ctx.save_for_backward(field)
-        ctx.handles = (hp, th)
         ctx.n = n
+        if ctx.needs_input_grad[0]:
+            ctx.save_for_backward(field)
+            ctx.handles = (key, hp, th)  # the pyramid of this forward, kept for the adjoint
+        else:
+            ctx.handles = None
+            _give_back(key, (hp, th))
         return pos, nrm
 
     @staticmethod
     @torch.autograd.function.once_differentiable
     def backward(ctx, gpos, gnrm):
         (field,) = ctx.saved_tensors
-        hp, th = ctx.handles
+        key, hp, th = ctx.handles
         dfield = torch.empty_strided(field.shape, field.stride(), dtype=torch.float32, device=field.device)
         dfield.zero_()
         if ctx.n:
             gp = None if gpos is None else gpos.to(torch.float32).contiguous()
             gn = None if gnrm is None else gnrm.to(torch.float32).contiguous()
+            hp.set_stream(torch.cuda.current_stream())
             th.adjoint(gp, gn, ctx.n, dfield)
-        th.close()
-        hp.close()
         ctx.handles = None
+        _give_back(key, (hp, th))
         return dfield, None, None, None
 
 

@@ -136,10 +136,11 @@ __device__ __forceinline__ uint32_t active_list_from_rows(uint32_t* list, const 
 // One warp: classify slice z of footprint (fx, fy) from sample-bit rows of the
 // lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Blocks with
 // vertices get their level-5 count and their active-cell list; s_codes is the
-// warp's 1 KiB staging area.
+// warp's 1 KiB staging area.  full: every cell of the footprint lies inside
+// the grid (vmask is all ones in every lane).
 __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, int lane,
-                                                    uint32_t vmask, const uint32_t* rows_b, uint64_t col_b,
-                                                    const uint32_t* rows_t, uint64_t col_t,
+                                                    uint32_t vmask, bool full, const uint32_t* rows_b,
+                                                    uint64_t col_b, const uint32_t* rows_t, uint64_t col_t,
                                                     const uint8_t* s_cnt, uint8_t* s_codes) {
     // rows y and y+1 of both layers; bit 32 of a row (column x0+32) comes
     // from the column word: (row >> 1) | colbit << 31 is the row shifted by one cell
@@ -147,6 +148,20 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
     const uint32_t ctl = (uint32_t)col_t, cth = (uint32_t)(col_t >> 32);
     const uint32_t a0 = rows_b[lane], a1 = rows_b[lane + 1];
     const uint32_t b0 = rows_t[lane], b1 = rows_t[lane + 1];
+    if (full && !V.codes_out) {
+        // A full block has no vertices iff its 33x33x2 samples all lie on one
+        // side of the iso-value (two samples that differ have some edge
+        // between them that differs, and every edge belongs to a cell of the
+        // block): one AND and one OR of the lane's two rows in both layers
+        // and of its two column bits, two votes.
+        const uint32_t cb = __funnelshift_r(cbl, cbh, lane) & 3u, ct = __funnelshift_r(ctl, cth, lane) & 3u;
+        const bool below_all = ((a0 & a1 & b0 & b1) == 0xffffffffu) && ((cb & ct) == 3u);
+        const bool above_all = ((a0 | a1 | b0 | b1) == 0u) && ((cb | ct) == 0u);
+        if (__all_sync(0xffffffffu, below_all) || __all_sync(0xffffffffu, above_all)) {
+            if (lane == 0) V.levels[V.level_off[kBlockLevel] + column_block_index(V, z, fx, fy)] = 0u;
+            return;
+        }
+    }
     uint32_t c[8];
     c[0] = a0;                                                   // (x,   y,   z)
     c[1] = (a0 >> 1) | (((cbl >> lane) & 1u) << 31);             // (x+1, y,   z)
@@ -259,14 +274,14 @@ __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st
 // the work rotates over the warps from box to box.  glu = running index of
 // the column's layer 0.
 __device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, int lb, int nl,
-                                                    uint32_t glu, int warp, int lane, uint32_t vmask,
+                                                    uint32_t glu, int warp, int lane, uint32_t vmask, bool full,
                                                     ColumnSmem& C) {
     // the slice of this warp, if any
     const int sl = lb - 1 + (int)(((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u);
     if (sl >= 0 && sl <= lb + nl - 2) {
         const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
-        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt], C.cnt,
-                            C.codes[warp]);
+        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, full, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt],
+                            C.cnt, C.codes[warp]);
     }
 }
 
@@ -320,6 +335,7 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         }
     }
     const uint32_t vmask = row_mask(V, x0, y0, lane);
+    const bool full = __all_sync(0xffffffffu, vmask == 0xffffffffu);
 
     bool timed_out = false;
     int k = 0;
@@ -341,7 +357,7 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
             tma_load_3d(s_ring + s * G::STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox,
                         &C.bar[s]);
         }
-        classify_box_slices(V, z0, fx, fy, lb, nl, 0u, warp, lane, vmask, C);
+        classify_box_slices(V, z0, fx, fy, lb, nl, 0u, warp, lane, vmask, full, C);
     }
     if (timed_out) {
         // drain the boxes still in flight (bounded) before the CTA exits
@@ -419,6 +435,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         column(u, fx, fy, z0, nlayers);
         const int nbox = (nlayers + kLayersPerBox - 1) / kLayersPerBox;
         const uint32_t vmask = row_mask(V, fx * 32, fy * 32, lane);
+        const bool full = __all_sync(0xffffffffu, vmask == 0xffffffffu);
         const uint32_t glu = pos * kLayersPerBox;
         for (int k = 0; k < nbox; k++, pos++) {
             const int s = (int)(pos % kRingStages);
@@ -435,7 +452,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
                 break;
             }
             if (tid == 0) issue_next();  // refill stage s
-            classify_box_slices(V, z0, fx, fy, lb, nl, glu, warp, lane, vmask, C);
+            classify_box_slices(V, z0, fx, fy, lb, nl, glu, warp, lane, vmask, full, C);
         }
     }
     if (timed_out && tid == 0) {

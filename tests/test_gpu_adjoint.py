@@ -165,3 +165,42 @@ def test_adjoint_uint8_field(hpmc, oracle):
     assert (err <= 1e-5 * S + 1e-9 * np.abs(g64).max()).all()
     th.close()
     hp.close()
+
+
+def test_autograd_handle_pool(hpmc, spheres):
+    """The autograd wrapper reuses pyramid handles per field shape: two
+    differentiable forwards of different fields in flight before either
+    backward each keep their own pyramid (their gradients equal those computed
+    one at a time, up to the atomics' summation order), and a forward without
+    gradients hands its handles back at once."""
+    import torch
+
+    from hpmc_b200 import autograd
+
+    field, iso = spheres
+    base = torch.from_numpy(field).cuda()
+    fields = [base, base * 1.1 + 0.002]
+
+    def loss_of(pos, nrm, seed):
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        w = torch.randn(pos.shape, generator=g).cuda()
+        u = torch.randn(nrm.shape, generator=g).cuda()
+        return (pos * w).sum() + (nrm * u).sum()
+
+    alone = []
+    for i, f in enumerate(fields):
+        x = f.clone().requires_grad_(True)
+        pos, nrm = autograd.extract(x, iso)
+        loss_of(pos, nrm, i).backward()
+        alone.append(x.grad.clone())
+    xs = [f.clone().requires_grad_(True) for f in fields]
+    outs = [autograd.extract(x, iso) for x in xs]  # both forwards before either backward
+    for i in (1, 0):
+        loss_of(*outs[i], i).backward()
+    for x, g in zip(xs, alone):
+        torch.testing.assert_close(x.grad, g, rtol=1e-5, atol=1e-6 * float(g.abs().max()))
+    key = (str(base.device), tuple(base.shape), base.dtype, tuple(base.stride()))
+    free = len(autograd._POOL[key])
+    with torch.no_grad():
+        autograd.extract(base, iso)
+    assert len(autograd._POOL[key]) == free  # borrowed and given back
