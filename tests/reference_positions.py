@@ -30,6 +30,18 @@ def printed_texel_constant(extract_glsl: str) -> float:
     return float(m.group(1))
 
 
+def shader_rounding(L, extent=(1.0, 1.0, 1.0)):
+    """Per-axis absolute bound of the FP32 rounding in the shader's tile
+    arithmetic: fract(foo) with foo up to the number of tiles loses up to an
+    ulp of that many tiles, scaled to world units by 2 tile / cells (x, y);
+    a few such ulps, as the position is rescaled twice afterwards."""
+    eps = 2.0 ** -24
+    cx, cy, _ = L.cells
+    tx, ty = L.tile
+    lx, ly = L.layout
+    return np.array([8 * eps * lx * 2 * tx * extent[0] / cx, 8 * eps * ly * 2 * ty * extent[1] / cy, 0.0])
+
+
 def reference_positions(L, cell, edge, t, edge_table, c_printed, extent=(1.0, 1.0, 1.0)):
     """(n, 3) positions of vertices (cell (x, y, z), MC edge, t) through the
     shader's tile arithmetic with the printed constant."""
