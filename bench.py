@@ -309,7 +309,11 @@ def run_batched(args, dev, stream, rank=0, world=1):
     pos = torch.empty((total, 4), dtype=torch.float32, device=dev)
     nrm = torch.empty_like(pos)
     with torch.cuda.stream(stream):
-        tuning = b.autotune(pos, nrm, total, stream=stream)
+        if args.batch_tuning:
+            b.set_tuning(*[int(v) for v in args.batch_tuning.split(",")])
+            tuning = b.tuning()
+        else:
+            tuning = b.autotune(pos, nrm, total, stream=stream)
         for _ in range(3):
             b.extract(pos, nrm, total, stream=stream)
         stream.synchronize()
@@ -667,6 +671,9 @@ def main():
     ap.add_argument("--lattice", type=int, default=512, help="lattice edge (profiling runs use smaller ones)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-extraction leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-extraction leg")
+    ap.add_argument("--batch-tuning", default="",
+                    help="fixed batch tuning 'column_slices,ctas_per_sm,rounds' instead of the autotuner "
+                         "(profiling runs)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world = int(os.environ.get("WORLD_SIZE", "1"))
