@@ -12,7 +12,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -35,6 +38,12 @@ constexpr int kRoundChoices[5] = {4, 8, 16, 32, 64};
 constexpr int kTraverseCtaChoices[3] = {2, 3, 4};
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Autotuner choices of this process per batch signature (scalar type, normal
+// mode, SM count and every volume's lattice): a later batch of the same shape
+// takes the choice without timing the 72 candidates again.
+std::mutex g_tune_mu;
+std::map<std::vector<long long>, std::array<int, 3>> g_tune_cache;
 
 }  // namespace
 
@@ -475,6 +484,20 @@ int HPMCbatchGetOffsets(HPMCBatch* b, unsigned long long* host_offsets) {
 int HPMCbatchAutotune(HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices, void* cuda_stream,
                       int chosen[3]) {
     if (!valid(b)) return HPMC_ERR_INVALID_HANDLE;
+    std::vector<long long> key{b->ftype, b->normal_mode, b->constants->num_sms, b->nvol};
+    for (const HPMCBatchVolume& v : b->src) key.insert(key.end(), {v.size[0], v.size[1], v.size[2]});
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            b->column_slices = it->second[0];
+            b->traverse_ctas_per_sm = it->second[1];
+            b->rounds = it->second[2];
+            apply_column_slices(b);
+            if (chosen) std::memcpy(chosen, it->second.data(), sizeof(int) * 3);
+            return HPMC_OK;
+        }
+    }
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
@@ -525,6 +548,10 @@ int HPMCbatchAutotune(HPMCBatch* b, float* positions, float* normals, size_t cap
     b->rounds = br;
     apply_column_slices(b);
     if (status != HPMC_OK) return status;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {bz, bc, br};
+    }
     if (chosen) {
         chosen[0] = bz;
         chosen[1] = bc;

@@ -369,7 +369,10 @@ int HPMCbatchGetTuning(struct HPMCBatch* b, int out[3]);
  * checked). */
 int HPMCbatchSetTestStall(struct HPMCBatch* b, int volume, int box, unsigned int wait_limit_us);
 /* Times every tuning choice on these outputs (graph replays, CUDA events)
- * and keeps the fastest; `chosen` (may be NULL) receives it. */
+ * and keeps the fastest; `chosen` (may be NULL) receives it.  The choice is
+ * remembered for the rest of the process per batch signature (scalar type,
+ * normal mode, SM count, every volume's lattice size): autotuning a batch of
+ * the same signature again takes it without timing. */
 int HPMCbatchAutotune(struct HPMCBatch* b, float* positions, float* normals, size_t capacity_vertices,
                       void* cuda_stream, int chosen[3]);
 

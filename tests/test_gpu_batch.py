@@ -199,3 +199,33 @@ def test_batch_64_uneven_volumes(hpmc):
         np.testing.assert_allclose(pos[offs[i]:offs[i + 1]], g["pos"], rtol=0, atol=1e-6)
         np.testing.assert_allclose(nrm[offs[i]:offs[i + 1]], g["nrm"], rtol=0, atol=1e-6)
     b.close()
+
+
+def test_autotune_choice_is_cached_per_signature(hpmc):
+    """A second batch with the same volumes, scalar type and normal mode takes
+    the first one's tuning without timing the candidates again."""
+    import time
+
+    import torch
+
+    from hpmc_b200 import datasets
+
+    vols = [datasets.metaballs(0, np.array([[0.5, 0.5, 0.5]]), np.array([0.2]), shape=(36 + 4 * i, 40, 44))
+            for i in range(5)]
+    fields = [torch.from_numpy(v).cuda() for v in vols]
+    cap = 200000
+    pos = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+    nrm = torch.empty_like(pos)
+    a = hpmc.Batch(fields, [1.0] * 5, normals=hpmc.NORMALS_CENTRAL)
+    t0 = time.perf_counter()
+    first = a.autotune(pos, nrm, cap)
+    t1 = time.perf_counter()
+    b = hpmc.Batch(fields, [1.0] * 5, normals=hpmc.NORMALS_CENTRAL)
+    second = b.autotune(pos, nrm, cap)
+    t2 = time.perf_counter()
+    assert second == first == b.tuning()
+    assert (t2 - t1) < 0.2 * (t1 - t0)
+    b.extract(pos, nrm, cap)
+    assert b.offsets()[-1] > 0
+    a.close()
+    b.close()
