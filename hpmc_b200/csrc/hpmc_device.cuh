@@ -74,7 +74,9 @@ struct Ctrl {
     unsigned int work_next;      // traversal work queue: next chunk to hand out
     unsigned int work_done;      // traversal CTAs finished (the last one resets the queue)
     unsigned int active_blocks;  // non-empty blocks of the last build
-    unsigned int pad;
+    unsigned int col_next;       // column classifier's work queue: next column to claim
+    unsigned int col_done;       // column classifier CTAs finished (the last one resets the queue)
+    unsigned int pad[2];
 };
 
 enum : unsigned int {

@@ -370,20 +370,23 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
     }
 }
 
-// Persistent column classifier: CTA b takes columns b, b + gridDim.x, ...
-// (column = footprint (fx, fy) x one run of column_slices slices, numbered
-// footprint-fastest so that neighbouring CTAs share halo samples in L2).
-// Thread 0 streams the boxes of the CTA's columns back to back through the
-// ring, so the copy engine never idles between columns.
+// Persistent column classifier (column = footprint (fx, fy) x one run of
+// column_slices slices, numbered footprint-fastest so that neighbouring
+// columns share halo samples in L2).  Thread 0 claims columns from a device
+// queue (one atomic per column: a CTA whose columns end early takes more) and
+// streams their boxes back to back through the ring, tagging every stage with
+// its column and box, so the copy engine never idles between columns; after
+// the last column it arrives on the next stage without a copy, tagged -1.
+// The last CTA to finish resets the queue for the next launch.
 template <int FT>
 __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_constant__ CUtensorMap tmap,
                                                              const __grid_constant__ Volume V, int ncolumns) {
     using G = ColumnGeom<FT>;
     uint8_t* const s_ring = ring_base<FT>();
     __shared__ __align__(16) ColumnSmem C;
+    __shared__ int2 s_tag[kRingStages];  // column and box of each ring stage (column -1: end)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int per_slab = V.nfx * V.nfy;
-    const int stride = (int)gridDim.x;
     const float iso = V.binary ? 0.5f : V.iso;
     const int u8_thr = V.u8_thr;
     // column u -> footprint, first slice, layers (slices + 1)
@@ -406,60 +409,83 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     // CTAs resident and waiting through the whole build measured ~2% slower).
     wait_prior_grid();
     __syncthreads();
-    // producer state (thread 0): next box to issue = box pk of column pu
-    int pu = blockIdx.x, pk = 0;
+    // producer state (thread 0): next box to issue = box pk of column pu; the
+    // following column is claimed one column ahead (pnext), so the atomic's
+    // round trip overlaps the current column
+    int pu = -1, pk = 0, pnl = 0, pz0 = 0, pfx = 0, pfy = 0, pnext = -1;
+    bool pdone = false;
     uint32_t issued = 0;
+    if (tid == 0) pnext = (int)atomicAdd(&V.ctrl->col_next, 1u);
     auto issue_next = [&]() {
-        if (pu >= ncolumns) return;
-        int fx, fy, z0, nl;
-        column(pu, fx, fy, z0, nl);
+        if (pdone) return;
         const int s = (int)(issued % kRingStages);
-        // test hook: CTA 0 never issues its box stall_box (its waits run out)
-        if (blockIdx.x != 0 || (int)issued != V.stall_box) {
+        if (pu < 0 || pk * kLayersPerBox >= pnl) {
+            pu = pnext;
+            if (pu < ncolumns) pnext = (int)atomicAdd(&V.ctrl->col_next, 1u);
+            pk = 0;
+            if (pu >= ncolumns) {
+                s_tag[s] = make_int2(-1, 0);
+                mbar_arrive(&C.bar[s]);  // completes the phase: the consumers see the end tag
+                issued++;
+                pdone = true;
+                return;
+            }
+            column(pu, pfx, pfy, pz0, pnl);
+        }
+        s_tag[s] = make_int2(pu, pk);
+        // test hook: a CTA never issues its box stall_box (its waits run out)
+        if ((int)issued != V.stall_box) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
-            tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, fx * 32, fy * 32, z0 + pk * kLayersPerBox, &C.bar[s]);
+            tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, pfx * 32, pfy * 32, pz0 + pk * kLayersPerBox, &C.bar[s]);
         }
         issued++;
-        if (++pk * kLayersPerBox >= nl) {
-            pk = 0;
-            pu += stride;
-        }
+        pk++;
     };
     if (tid == 0)
         for (int i = 0; i < kRingStages; i++) issue_next();
 
     bool timed_out = false;
     uint32_t pos = 0;  // running box position (ring slot, phase, row-buffer index)
-    for (int u = blockIdx.x; u < ncolumns && !timed_out; u += stride) {
-        int fx, fy, z0, nlayers;
-        column(u, fx, fy, z0, nlayers);
-        const int nbox = (nlayers + kLayersPerBox - 1) / kLayersPerBox;
+    for (;; pos++) {
+        const int s = (int)(pos % kRingStages);
+        const uint32_t parity = (pos / kRingStages) & 1u;
+        const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
+        // the stage's tag was written before the producer's arrival (release) on its barrier
+        const int2 tag = ok ? s_tag[s] : make_int2(-1, 0);
+        int fx = 0, fy = 0, z0 = 0, nlayers = 0;
+        if (tag.x >= 0) column(tag.x, fx, fy, z0, nlayers);
+        const int k = tag.y;
+        const int lb = k * kLayersPerBox;
+        const int nl = min(kLayersPerBox, nlayers - lb);
+        if (ok && tag.x >= 0)
+            convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl,
+                            pos * kLayersPerBox, iso, u8_thr, warp, lane, C);
+        // the only CTA barrier of a box (uniform decision on a timed-out wait);
+        // the producer rewrites the stage and its tag only after it
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        if (tag.x < 0) break;        // the end tag (the same for every thread)
+        if (tid == 0) issue_next();  // refill stage s
         const uint32_t vmask = row_mask(V, fx * 32, fy * 32, lane);
         const bool full = __all_sync(0xffffffffu, vmask == 0xffffffffu);
-        const uint32_t glu = pos * kLayersPerBox;
-        for (int k = 0; k < nbox; k++, pos++) {
-            const int s = (int)(pos % kRingStages);
-            const uint32_t parity = (pos / kRingStages) & 1u;
-            const int lb = k * kLayersPerBox;
-            const int nl = min(kLayersPerBox, nlayers - lb);
-            const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
-            if (ok)
-                convert_box<FT>(reinterpret_cast<const typename G::T*>(s_ring + s * G::STAGE_STRIDE), nl,
-                                pos * kLayersPerBox, iso, u8_thr, warp, lane, C);
-            // the only CTA barrier of a box (uniform decision on a timed-out wait)
-            if (__syncthreads_or(!ok)) {
-                timed_out = true;
-                break;
-            }
-            if (tid == 0) issue_next();  // refill stage s
-            classify_box_slices(V, z0, fx, fy, lb, nl, glu, warp, lane, vmask, full, C);
-        }
+        classify_box_slices(V, z0, fx, fy, lb, nl, (pos - (uint32_t)k) * kLayersPerBox, warp, lane, vmask, full, C);
     }
     if (timed_out && tid == 0) {
         // drain the boxes still in flight (bounded) before the CTA exits
         for (uint32_t p = pos; p < issued; p++)
             mbar_wait_bounded(&C.bar[p % kRingStages], (p / kRingStages) & 1u, V.wait_limit_ns, nullptr, 0u);
         atomicOr(&V.ctrl->status, kStatusTimeout);
+    }
+    // the last CTA to finish resets the column queue for the next launch
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&V.ctrl->col_done, 1u) == gridDim.x - 1) {
+            V.ctrl->col_next = 0;
+            V.ctrl->col_done = 0;
+            __threadfence();
+        }
     }
 }
 

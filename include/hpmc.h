@@ -254,9 +254,10 @@ int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
 
 /* Test hook for failure detection (no counterpart in the reference; it
  * makes a bounded device wait run out without any fault).  From the next
- * build on, the TMA column classifier's producer never issues box `box`
- * (0-based) of its first column -- neither the expected-byte count nor the
- * copy -- so the consumers' waits on that box give up after wait_limit_us
+ * build on, the producer of every persistent TMA column classifier CTA never
+ * issues box `box` (0-based) of the CTA's stream of boxes -- neither the
+ * expected-byte count nor the copy -- so the consumers' waits on that box
+ * give up after wait_limit_us
  * microseconds (0: the default limit of 2 s), the CTAs drain their copies
  * in flight and exit, and the build reports HPMC_ERR_TIMEOUT
  * (HPMCacquireNumberOfVertices returns 0 and breaks the handle).  box < 0

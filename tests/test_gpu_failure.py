@@ -43,7 +43,7 @@ def test_handle_build_timeout_is_reported_and_recoverable(hpmc, oracle):
     nrm = torch.zeros_like(pos)
     th.set_buffers(pos, nrm, n_ok)
 
-    # at 96^3 every persistent CTA streams one one-box column: box 0 is CTA 0's
+    # at 96^3 every persistent CTA streams one one-box column: each skips its box 0
     hp.set_test_stall(0, WAIT_US)
     hp.build(iso)
     assert hp.acquire_number_of_vertices() == 0
@@ -76,8 +76,9 @@ def test_timeout_of_a_later_box_and_the_device_status(hpmc):
     hp = hpmc.HistoPyramid(hpmc.default_constants())
     hp.set_stream(torch.cuda.current_stream())
     hp.set_field_device(field)
-    # at 256^3 CTA 0 streams 8 one-box columns back to back: its box 5 comes
-    # after several refills of the two ring slots
+    # at 256^3 2,368 one-box columns are shared by 296 persistent CTAs, so
+    # some CTA streams at least 8 boxes: its box 5 comes after several refills
+    # of the two ring slots
     hp.set_test_stall(5, WAIT_US)
     hp.build(iso)
     torch.cuda.synchronize()
