@@ -912,7 +912,7 @@ extern "C" int HPMCextractStatic(const void* field, int scalar_type, GLsizei x_s
     hpmc::host::volume_layout(V, lattice, cells, ext, L, &level_entries_total, &slots);
     V.column_slices = hpmc::host::default_column_slices(V, dev->num_sms);
 
-    // carve the scratch: control block | dense levels | active-cell lists
+    // carve the scratch: control block | dense levels | block codes
     const size_t ctrl_bytes = align256(sizeof(Ctrl));
     const size_t levels_bytes = align256(sizeof(uint32_t) * (size_t)level_entries_total);
     const size_t arena_bytes = hpmc::kSlotBytes * (size_t)slots;

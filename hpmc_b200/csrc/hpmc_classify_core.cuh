@@ -56,8 +56,8 @@ __device__ __forceinline__ void write_codes(const Volume& V, uint32_t packed, in
 // Generic classification: CTA = one 32x32 block of the virtual cell grid,
 // for any tiling (tiles narrower than 32 cells), unaligned pitches and
 // functor fields.  Each thread loads its quad's 3x3x2 samples directly; the
-// quads are numbered in Morton order, so the block's active-cell list comes
-// from one block-wide scan.
+// quads are numbered in Morton order, so thread t's four codes are word t of
+// the block's arena slot.
 template <int FT, class UF = NoUserField>
 __device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b, uint8_t* s_cnt,
                                                     uint32_t* s_warp) {
@@ -91,48 +91,19 @@ __device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b,
             if (V.codes_out) write_codes(V, packed, x, y, z);
         }
     }
-    // thread = quad = cells 4 tid .. 4 tid + 3 in Morton order: its active
-    // cells and vertices, one block-wide scan for list slots and first vertices
-    uint32_t vs = 0, na = 0;
+    // thread = quad = cells 4 tid .. 4 tid + 3 in Morton order: its vertices,
+    // one block reduction for the block's count
+    uint32_t vs = 0;
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const uint32_t n = s_cnt[(packed >> (8 * c)) & 0xffu];
-        vs += n;
-        na += n ? 1u : 0u;
-    }
-    const uint32_t mine = vs | (na << 16);
-    uint32_t inc = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_warp[warp] = inc;
+    for (int c = 0; c < 4; c++) vs += s_cnt[(packed >> (8 * c)) & 0xffu];
+    vs = __reduce_add_sync(0xffffffffu, vs);
+    if (lane == 0) s_warp[warp] = vs;
     __syncthreads();
-    uint32_t off = 0, all = 0;
+    uint32_t total = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; w++) {
-        const uint32_t t = s_warp[w];
-        if (w < warp) off += t;
-        all += t;
-    }
-    const uint32_t total = all & 0xffffu;
+    for (int w = 0; w < kWarps; w++) total += s_warp[w];
     if (tid == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-    if (total) {
-        uint32_t* list = V.arena + block_slot(V, b) * kSlotWords;
-        const uint32_t excl = off + inc - mine;
-        uint32_t vpos = excl & 0xffffu, apos = excl >> 16;
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const uint32_t code = (packed >> (8 * c)) & 0xffu;
-            const uint32_t n = s_cnt[code];
-            if (n) {
-                list[apos++] = (vpos << kListStartShift) | (code << 10) | (4u * (uint32_t)tid + (uint32_t)c);
-                vpos += n;
-            }
-        }
-        if (tid < kListSentinels) list[(all >> 16) + (uint32_t)tid] = kListSentinel;
-    }
+    if (total) V.arena[block_slot(V, b) * kSlotWords + tid] = packed;
     __syncthreads();
 }
 

@@ -15,10 +15,12 @@
 //     count as uint32 -- level j equals the reference's mip level j flattened
 //     channel by channel (level j texel t, channel c <-> entry 4*morton(t)+c);
 //   * below block level nothing is stored densely: each block with a non-zero
-//     count gets an "arena" slot holding its active-cell list -- the cells
-//     with vertices, in Morton (= vertex) order, each with its MC code and the
+//     count gets an "arena" slot holding its 1024 MC codes in Morton order.
+//     A traversal warp that enters the block turns them into the block's
+//     active-cell list in its own shared memory -- the cells with vertices,
+//     in Morton (= vertex) order, each with its MC code and the
 //     block-relative index of its first vertex.  Levels 0..4 of the reference
-//     are thus implied by the lists: the count of a Morton range of cells is
+//     are thus implied by the codes: the count of a Morton range of cells is
 //     the difference of two list starts.  Cells of empty blocks are all
 //     inside or all outside and are not needed.
 #pragma once
@@ -33,8 +35,13 @@ constexpr int kBlockLevel = 5;       // 4^5 keys per block
 constexpr int kBlockKeys = 1024;
 constexpr int kMaxLevels = 40;
 
-// Active-cell list of one block (one arena slot): one word per cell with
-// vertices, in Morton order,
+// Arena slot of a non-empty block: its codes in Morton order, four per word
+// (cell 4i + c in byte c of word i).
+constexpr int kSlotWords = kBlockKeys / 4;
+constexpr size_t kSlotBytes = sizeof(uint32_t) * (size_t)kSlotWords;
+
+// Active-cell list of one block (a traversal warp's shared memory): one word
+// per cell with vertices, in Morton order,
 //     start << 18 | code << 10 | cell
 // start = block-relative index of the cell's first vertex (< 15 * 1024),
 // code = MC case, cell = Morton index of the cell in the block.  The last
@@ -42,8 +49,7 @@ constexpr int kMaxLevels = 40;
 // any vertex), so a warp may read the 32 entries after any list position
 // without knowing the list's length.
 constexpr int kListSentinels = 32;
-constexpr int kSlotWords = kBlockKeys + kListSentinels;
-constexpr size_t kSlotBytes = sizeof(uint32_t) * (size_t)kSlotWords;
+constexpr int kListWords = kBlockKeys + kListSentinels;
 constexpr uint32_t kListSentinel = 0xffffffffu;
 constexpr int kListStartShift = 18;
 
@@ -73,10 +79,9 @@ struct Ctrl {
     unsigned int written;        // vertices written by the last extraction
     unsigned int work_next;      // traversal work queue: next chunk to hand out
     unsigned int work_done;      // traversal CTAs finished (the last one resets the queue)
-    unsigned int active_blocks;  // non-empty blocks of the last build
     unsigned int col_next;       // column classifier's work queue: next column to claim
     unsigned int col_done;       // column classifier CTAs finished (the last one resets the queue)
-    unsigned int pad[2];
+    unsigned int pad[3];
 };
 
 enum : unsigned int {
@@ -129,7 +134,7 @@ struct Volume {
     int column_layout;
     int nfx, nfy;                      // 32-cell footprints per slice in x, y
     int column_slices;                 // slices per column CTA
-    uint32_t* arena;                   // kSlotWords words (one active-cell list) per slot
+    uint32_t* arena;                   // kSlotWords words (one block's codes) per slot
     long long arena_slots;             // capacity of the arena
     Ctrl* ctrl;
     // optional capture of every cell's code, [cz][cy][cx] (inspection)

@@ -34,6 +34,7 @@ enum { kModeForward = kGeomForward, kModeCentral = kGeomCentral, kModeBinary = k
 namespace {
 
 struct TraverseSmem {
+    uint32_t list[kWarps][kListWords];  // per warp: the active-cell list of the block it is in
     uint64_t edge[256];
     uint32_t top[kTopCacheEntries];
     uint16_t morton[kBlockKeys];  // cell Morton index in a block -> cx | cy << 8
@@ -46,21 +47,68 @@ constexpr size_t kBatchSmem = kBatchVolOffset + kWarps * sizeof(Volume);
 
 // The block a warp is working in: its key-space origin and, for the column
 // layout, the lattice cell of its first key (every cell of such a block lies
-// in the same slice tile); its active-cell list and the list entry of the
-// cell holding the next block-relative vertex the warp expects (knext).
+// in the same slice tile); its active-cell list (the warp's shared-memory
+// area) and the list entry of the cell holding the next block-relative
+// vertex the warp expects (knext).
 struct WarpBlock {
     uint32_t b, base, count;
     uint32_t X0, Y0;
     int ox, oy, oz;
-    const uint32_t* list;
+    uint32_t* list;
     uint32_t cur, knext;
     bool have;
 };
 
-// List entry j of a block (clamped to the slot: consistent data never reads
-// past the sentinels that follow the last entry).
+// List entry j of a block (clamped to the list area: consistent data never
+// reads past the sentinels that follow the last entry).
 __device__ __forceinline__ uint32_t list_entry(const uint32_t* list, uint32_t j) {
-    return __ldg(list + (j < (uint32_t)kSlotWords ? j : (uint32_t)(kSlotWords - 1)));
+    return list[j < (uint32_t)kListWords ? j : (uint32_t)(kListWords - 1)];
+}
+
+// One warp: block b's active-cell list into `list` from its arena slot (1024
+// codes in Morton order, one slot word per quad).  Lane l takes the codes of
+// Morton cells 32l .. 32l+31 (two 16-byte loads) and counts their vertices
+// (32 independent table reads); one warp scan of (cells << 16 | vertices)
+// gives every lane its first list entry and first vertex, and the lane
+// writes its active cells in order.  32 sentinels follow the last entry.
+__device__ __forceinline__ void load_block(const Volume& V, const uint8_t* s_cnt, uint32_t* list, int lane,
+                                           uint32_t b) {
+    long long slot = block_slot(V, b);
+    slot = slot < V.arena_slots ? slot : V.arena_slots - 1;  // in range for consistent data
+    const uint4* src = reinterpret_cast<const uint4*>(V.arena + slot * kSlotWords) + 2 * lane;
+    const uint4 w0 = __ldg(src), w1 = __ldg(src + 1);
+    const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    uint32_t vsum = 0, amask = 0;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        const uint32_t c = s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        vsum += c;
+        if (c) amask |= 1u << i;
+    }
+    // block totals < 2^16 each
+    const uint32_t mine = vsum | ((uint32_t)__popc(amask) << 16);
+    uint32_t scan = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
+        if (lane >= o) scan += t;
+    }
+    const uint32_t excl = scan - mine;
+    uint32_t vpos = excl & 0xffffu, apos = excl >> 16;
+    __syncwarp();  // every lane is done with the previous list
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        uint32_t am = (amask >> (4 * k)) & 0xfu;
+        while (am) {
+            const int j = __ffs(am) - 1;
+            am &= am - 1u;
+            const uint32_t code = (w[k] >> (8 * j)) & 0xffu;
+            list[apos++] = (vpos << kListStartShift) | (code << 10) | (uint32_t)(32 * lane + 4 * k + j);
+            vpos += s_cnt[code];
+        }
+    }
+    list[(__shfl_sync(0xffffffffu, scan, 31) >> 16) + (uint32_t)lane] = kListSentinel;
+    __syncwarp();  // the list is visible to the warp
 }
 
 __device__ __forceinline__ uint32_t compact32(uint32_t v) {
@@ -138,10 +186,9 @@ struct VertexCell {
 
 // Block B.b with base B.base and count B.count found: its active-cell list
 // and the warp's position at block-relative vertex key - B.base.
-__device__ __forceinline__ void open_block(const Volume& V, int lane, uint32_t key, WarpBlock& B) {
-    long long slot = block_slot(V, B.b);
-    slot = slot < V.arena_slots ? slot : V.arena_slots - 1;  // in range for consistent data
-    B.list = V.arena + slot * kSlotWords;
+__device__ __forceinline__ void open_block(const Volume& V, const TraverseSmem& S, int lane, uint32_t key,
+                                           WarpBlock& B) {
+    load_block(V, S.cnt, B.list, lane, B.b);
     B.X0 = compact32(B.b) << 5;
     B.Y0 = compact32(B.b >> 1) << 5;
     virtual_to_cell(V, B.X0, B.Y0, B.ox, B.oy, B.oz);
@@ -154,7 +201,7 @@ __device__ __forceinline__ void open_block(const Volume& V, int lane, uint32_t k
 __device__ __forceinline__ void enter_block(const Volume& V, const TraverseSmem& S, int lane, uint32_t key,
                                             WarpBlock& B) {
     descend(V, S, key, B.b, B.base, B.count);  // uniform across the warp
-    open_block(V, lane, key, B);
+    open_block(V, S, lane, key, B);
 }
 
 // A warp walking forward out of block B.b: the next block with vertices, if
@@ -189,7 +236,7 @@ __device__ __forceinline__ bool resolve_vertex(const Volume& V, const TraverseSm
         const uint32_t vl = __shfl_sync(0xffffffffu, v, leader);
         if (!B.have || vl < B.base || vl - B.base >= B.count) {
             if (B.have && vl - B.base == B.count && next_sibling(V, lane, B))
-                open_block(V, lane, vl, B);
+                open_block(V, S, lane, vl, B);
             else
                 enter_block(V, S, lane, vl, B);
         } else if (vl - B.base != B.knext) {
@@ -323,6 +370,7 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
     const uint32_t nchunks = (N + VW - 1) / VW;
     WarpBlock B;
     B.have = false;
+    B.list = S.list[warp];
     for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
         for (uint32_t r = 0; r < rounds; r++) {

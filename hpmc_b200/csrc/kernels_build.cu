@@ -35,9 +35,16 @@ namespace hpmc {
 // k = bit k (dx + 2dy + 4dz) of the 32 codes.  AND/OR over the eight words
 // marks the cells that are neither all-inside nor all-outside (the only ones
 // with vertices); only those go through the count table.  The warp sum is the
-// block's level-5 entry; non-empty blocks also store their active-cell list
-// (Morton order, with codes and first vertices) in the arena, so that the
-// traversal never re-reads codes or recounts a block.
+// block's level-5 entry; non-empty blocks also store their 1024 codes in
+// Morton order in their arena slot (1 KiB), from which a traversal warp
+// builds the block's active-cell list when it enters the block.
+//
+// Measured alternatives for the list: written by the classifier (each
+// non-empty block's serial gathers stall the box barrier: +20 us at 512^3),
+// or by a separate pass over queued slots beside the reduction (issue-bound,
+// ~500 warp instructions per list, not hidden by the 7 us reduction tree:
+// +11 us) -- both slower than one build per warp in the traversal, where the
+// latency of the list's gathers overlaps other warps' vertex work.
 namespace {
 
 template <int FT, typename T>
@@ -73,75 +80,15 @@ __device__ __forceinline__ void slices_to_codes(const uint32_t c[8], uint32_t w[
     }
 }
 
-// 16 bits -> Morton positions of an 8x2 cell tile: bit x of the low byte goes
-// to bit (x0 | x1 << 2 | x2 << 4), bit x of the high byte to that + 8.
-__device__ __forceinline__ uint32_t spread16(uint32_t t) {
-    t = (t | (t << 12)) & 0x0F0F0F0Fu;
-    return (t | (t << 2)) & 0x33333333u;
-}
-
-// One warp: the active-cell list of a 32x32 block (lane = row y) into `list`
-// (one arena slot), from the row's 32 codes (w[i] = cells 4i..4i+3) and its
-// active-cell mask.  Lane q then owns the Morton range 32q .. 32q+31, an 8x4
-// cell tile (Morton bits x0 y0 x1 y1 x2 | y2 x3 y3 x4 y4): it gathers the
-// tile's active bits from four rows into one Morton-ordered word, reads the
-// codes of those cells from the staged rows, and one warp scan gives every
-// lane its first list slot and first vertex.  Returns the block's vertices.
-__device__ __forceinline__ uint32_t active_list_from_rows(uint32_t* list, const uint32_t w[8], uint32_t active,
-                                                          int lane, uint8_t* s_codes, const uint8_t* s_cnt) {
-    uint4* row = reinterpret_cast<uint4*>(s_codes + 32 * lane);
-    row[0] = make_uint4(w[0], w[1], w[2], w[3]);
-    row[1] = make_uint4(w[4], w[5], w[6], w[7]);
-    const uint32_t q = (uint32_t)lane;
-    const uint32_t y0 = 4u * ((q & 1u) | ((q >> 1) & 2u) | ((q >> 2) & 4u));
-    const uint32_t x0 = 8u * (((q >> 1) & 1u) | ((q >> 2) & 2u));
-    const uint32_t r0 = (__shfl_sync(0xffffffffu, active, (int)y0) >> x0) & 0xffu;
-    const uint32_t r1 = (__shfl_sync(0xffffffffu, active, (int)y0 + 1) >> x0) & 0xffu;
-    const uint32_t r2 = (__shfl_sync(0xffffffffu, active, (int)y0 + 2) >> x0) & 0xffu;
-    const uint32_t r3 = (__shfl_sync(0xffffffffu, active, (int)y0 + 3) >> x0) & 0xffu;
-    // rows 0/2 on Morton bit 3 = 0/1 with bit 1 = 0; rows 1/3 shifted by 2 (bit 1 = 1)
-    const uint32_t word = spread16(r0 | (r2 << 8)) | (spread16(r1 | (r3 << 8)) << 2);
-    __syncwarp();  // the staged rows are visible to the warp
-    uint32_t vsum = 0;
-    for (uint32_t m = word; m; m &= m - 1u) {
-        const uint32_t r = (uint32_t)(__ffs(m) - 1);
-        const uint32_t x = x0 + ((r & 1u) | ((r >> 1) & 2u) | ((r >> 2) & 4u));
-        const uint32_t y = y0 + (((r >> 1) & 1u) | ((r >> 2) & 2u));
-        vsum += s_cnt[s_codes[32u * y + x]];
-    }
-    // one scan of (active cells << 16 | vertices); both < 2^16 per block
-    const uint32_t mine = vsum | ((uint32_t)__popc(word) << 16);
-    uint32_t scan = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, scan, o);
-        if (lane >= o) scan += t;
-    }
-    const uint32_t all = __shfl_sync(0xffffffffu, scan, 31);
-    const uint32_t excl = scan - mine;
-    uint32_t vpos = excl & 0xffffu, apos = excl >> 16;
-    for (uint32_t m = word; m; m &= m - 1u) {
-        const uint32_t r = (uint32_t)(__ffs(m) - 1);
-        const uint32_t x = x0 + ((r & 1u) | ((r >> 1) & 2u) | ((r >> 2) & 4u));
-        const uint32_t y = y0 + (((r >> 1) & 1u) | ((r >> 2) & 2u));
-        const uint32_t code = s_codes[32u * y + x];
-        list[apos++] = (vpos << kListStartShift) | (code << 10) | (32u * q + r);
-        vpos += s_cnt[code];
-    }
-    list[(all >> 16) + (uint32_t)lane] = kListSentinel;
-    __syncwarp();  // the staged rows are free for the next block
-    return all & 0xffffu;
-}
-
 // One warp: classify slice z of footprint (fx, fy) from sample-bit rows of the
-// lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Blocks with
-// vertices get their level-5 count and their active-cell list; s_codes is the
-// warp's 1 KiB staging area.  full: every cell of the footprint lies inside
-// the grid (vmask is all ones in every lane).
+// lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Every block
+// gets its level-5 count; blocks with vertices store their codes in Morton
+// order in their slot.  full: every cell of the footprint lies inside the
+// grid (vmask is all ones in every lane).
 __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, int lane,
                                                     uint32_t vmask, bool full, const uint32_t* rows_b,
                                                     uint64_t col_b, const uint32_t* rows_t, uint64_t col_t,
-                                                    const uint8_t* s_cnt, uint8_t* s_codes) {
+                                                    const uint8_t* s_cnt) {
     // rows y and y+1 of both layers; bit 32 of a row (column x0+32) comes
     // from the column word: (row >> 1) | colbit << 31 is the row shifted by one cell
     const uint32_t cbl = (uint32_t)col_b, cbh = (uint32_t)(col_b >> 32);
@@ -192,9 +139,38 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
     uint32_t w[8];
     slices_to_codes(c, w);
     if (has_vertices) {
-        const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
-        const uint32_t total = active_list_from_rows(V.arena + slot * kSlotWords, w, active, lane, s_codes, s_cnt);
+        // the block's vertices: 32 independent count lookups per lane, one
+        // warp reduction (inactive cells have codes 0 or 255, count 0)
+        uint32_t vs = 0;
+#pragma unroll
+        for (int i = 0; i < 32; i++) vs += s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        const uint32_t total = __reduce_add_sync(0xffffffffu, vs);
         if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
+        // codes in Morton order: word q of the slot = quad (qx, qy), cells
+        // (2qx,2qy), (2qx+1,2qy), (2qx,2qy+1), (2qx+1,2qy+1) from rows 2qy
+        // (even lane) and 2qy+1 (odd lane); even lanes store qx 0..7, odd
+        // lanes qx 8..15, each pairing its row with its neighbour's
+        uint32_t p[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) p[i] = __shfl_xor_sync(0xffffffffu, w[i], 1);
+        const bool odd = lane & 1;
+        const uint32_t qy = (uint32_t)lane >> 1;
+        const long long slot = ((long long)z * V.nfy + fy) * V.nfx + fx;
+        uint32_t* dst = V.arena + slot * kSlotWords;
+        // Morton index of quad (qx, qy), qx = (odd ? 8 : 0) + i: the bits of i
+        // (compile-time) and of the lane's part are disjoint
+        const uint32_t qys = (qy & 1u) | ((qy & 2u) << 1) | ((qy & 4u) << 2) | ((qy & 8u) << 3);
+        const uint32_t qbase = (odd ? 0x40u : 0u) | (qys << 1);
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const uint32_t wi = odd ? w[4 + (i >> 1)] : w[i >> 1];  // this lane's word with cells 2qx, 2qx+1
+            const uint32_t pi = odd ? p[4 + (i >> 1)] : p[i >> 1];
+            const uint32_t upper = odd ? wi : pi;  // row 2qy+1
+            const uint32_t lower = odd ? pi : wi;  // row 2qy
+            const uint32_t word = __byte_perm(lower, upper, (i & 1) ? 0x7632 : 0x5410);
+            const uint32_t ispread = (uint32_t)((i & 1) | ((i & 2) << 1) | ((i & 4) << 2));
+            dst[qbase | ispread] = word;
+        }
     }
     if (V.codes_out) {
         const int y = fy * 32 + lane;
@@ -233,10 +209,8 @@ struct ColumnSmem {
     uint64_t col[kRowBuffers];                   // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
     uint64_t bar[kRingStages];
     uint8_t cnt[256];
-    alignas(16) uint8_t codes[kWarps][32 * 32];  // per warp: the codes of the block it lists
 };
 static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4 row stores need 16-byte alignment");
-static_assert(offsetof(ColumnSmem, codes) % 16 == 0, "uint4 code stores need 16-byte alignment");
 
 // Bit rows of the nl layers of one box (stage st), layer l stored at
 // running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
@@ -281,7 +255,7 @@ __device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int
     if (sl >= 0 && sl <= lb + nl - 2) {
         const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
         classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, full, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt],
-                            C.cnt, C.codes[warp]);
+                            C.cnt);
     }
 }
 
@@ -384,7 +358,10 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     using G = ColumnGeom<FT>;
     uint8_t* const s_ring = ring_base<FT>();
     __shared__ __align__(16) ColumnSmem C;
-    __shared__ int2 s_tag[kRingStages];  // column and box of each ring stage (column -1: end)
+    // per ring stage: box k | layers << 16 of its column (-1: end), footprint
+    // (fx, fy) and first slice -- decoded once by the producer, so that the
+    // consumers start converting without integer divisions after each wait
+    __shared__ int4 s_tag[kRingStages];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int per_slab = V.nfx * V.nfy;
     const float iso = V.binary ? 0.5f : V.iso;
@@ -424,7 +401,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             if (pu < ncolumns) pnext = (int)atomicAdd(&V.ctrl->col_next, 1u);
             pk = 0;
             if (pu >= ncolumns) {
-                s_tag[s] = make_int2(-1, 0);
+                s_tag[s] = make_int4(-1, 0, 0, 0);
                 mbar_arrive(&C.bar[s]);  // completes the phase: the consumers see the end tag
                 issued++;
                 pdone = true;
@@ -432,7 +409,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             }
             column(pu, pfx, pfy, pz0, pnl);
         }
-        s_tag[s] = make_int2(pu, pk);
+        s_tag[s] = make_int4(pk | (pnl << 16), pfx, pfy, pz0);
         // test hook: a CTA never issues its box stall_box (its waits run out)
         if ((int)issued != V.stall_box) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
@@ -451,10 +428,9 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         const uint32_t parity = (pos / kRingStages) & 1u;
         const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
         // the stage's tag was written before the producer's arrival (release) on its barrier
-        const int2 tag = ok ? s_tag[s] : make_int2(-1, 0);
-        int fx = 0, fy = 0, z0 = 0, nlayers = 0;
-        if (tag.x >= 0) column(tag.x, fx, fy, z0, nlayers);
-        const int k = tag.y;
+        const int4 tag = ok ? s_tag[s] : make_int4(-1, 0, 0, 0);
+        const int fx = tag.y, fy = tag.z, z0 = tag.w;
+        const int k = tag.x & 0xffff, nlayers = tag.x >> 16;
         const int lb = k * kLayersPerBox;
         const int nl = min(kLayersPerBox, nlayers - lb);
         if (ok && tag.x >= 0)

@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(kThreads, 4) adjoint_kernel(const __grid_const
     const uint32_t nchunks = (N + VW - 1) / VW;
     WarpBlock B;
     B.have = false;
+    B.list = S.list[warp];
     for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
         for (uint32_t r = 0; r < rounds; r++) {
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_batch(const __grid_const
     unsigned long long vb = 0;
     WarpBlock B;
     B.have = false;
+    B.list = S.list[warp];
     for (uint32_t item = next_chunk_batch(Bt, lane); item < nitems; item = next_chunk_batch(Bt, lane)) {
         if (cur < 0 || item < c0 || item >= c1) {
             const int v = find_segment(Bt.chunk_start, Bt.nvol, item);
@@ -249,6 +251,7 @@ __global__ void __launch_bounds__(kThreads, 4) mesh_keys(const __grid_constant__
     const uint32_t nchunks = (N + VW - 1) / VW;
     WarpBlock B;
     B.have = false;
+    B.list = S.list[warp];
     for (uint32_t chunk = next_chunk(V, lane); chunk < nchunks; chunk = next_chunk(V, lane)) {
 #pragma unroll 1
         for (uint32_t r = 0; r < rounds; r++) {
@@ -476,6 +479,21 @@ cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mo
 
 cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode, int grid, cudaStream_t st) {
     const bool central = normal_mode == kNormalsCentral;
+    // the adjoint's static cotangent buffer plus the traversal's dynamic
+    // shared memory pass the 48 KB a launch gets without opting in
+    static const bool opted_in = [] {
+        const int bytes = (int)kTraverseSmem;
+        cudaFuncSetAttribute(adjoint_kernel<kFieldF32, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(adjoint_kernel<kFieldF32, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(adjoint_kernel<kFieldU8, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(adjoint_kernel<kFieldU8, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(adjoint_kernel<kFieldUNorm8, kModeCentral>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
+        cudaFuncSetAttribute(adjoint_kernel<kFieldUNorm8, kModeForward>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes);
+        return true;
+    }();
+    (void)opted_in;
     switch (V.ftype) {
         case kFieldF32:
             if (central) adjoint_kernel<kFieldF32, kModeCentral><<<grid, kThreads, kTraverseSmem, st>>>(V, A);

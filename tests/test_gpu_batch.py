@@ -217,10 +217,12 @@ def test_autotune_choice_is_cached_per_signature(hpmc):
     pos = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
     nrm = torch.empty_like(pos)
     a = hpmc.Batch(fields, [1.0] * 5, normals=hpmc.NORMALS_CENTRAL)
+    b = hpmc.Batch(fields, [1.0] * 5, normals=hpmc.NORMALS_CENTRAL)
+    torch.cuda.synchronize()
+    # only the two autotune calls are timed (creating a batch allocates)
     t0 = time.perf_counter()
     first = a.autotune(pos, nrm, cap)
     t1 = time.perf_counter()
-    b = hpmc.Batch(fields, [1.0] * 5, normals=hpmc.NORMALS_CENTRAL)
     second = b.autotune(pos, nrm, cap)
     t2 = time.perf_counter()
     assert second == first == b.tuning()
