@@ -219,27 +219,37 @@ template <int FT>
 __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st, int nl, uint32_t gl0, float iso,
                                             int u8_thr, int warp, int lane, ColumnSmem& C) {
     using G = ColumnGeom<FT>;
+    using T = typename G::T;
+    // Every sample first, then the ballots and stores: the compiler cannot
+    // tell the bit-row stores from the ring stage, so loads issued after a
+    // store would wait for it.  A stage always holds kLayersPerBox layers
+    // (copies past the volume read zeros), so all of them are read; layers
+    // past nl are not stored.
+    T v[kLayersPerBox][4];
+    const T* row = st + 4 * warp * G::BXE + lane;
+#pragma unroll
+    for (int l = 0; l < kLayersPerBox; l++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[l][i] = row[l * G::LAYER + i * G::BXE];
+    const int le = (int)(((uint32_t)warp - gl0 - 3u) & 7u);  // the layer whose row 32 and column 32 this warp takes
+    const T* layer = st + le * G::LAYER;
+    const T e_row = layer[32 * G::BXE + lane], e_col = layer[lane * G::BXE + 32], e_corner = layer[32 * G::BXE + 32];
 #pragma unroll
     for (int l = 0; l < kLayersPerBox; l++) {
-        if (l < nl) {
-            const typename G::T* layer = st + l * G::LAYER;
-            const uint32_t buf = (gl0 + l) & (kRowBuffers - 1);
-            const typename G::T* row = layer + 4 * warp * G::BXE + lane;
-            const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(row[0], iso, u8_thr));
-            const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(row[G::BXE], iso, u8_thr));
-            const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(row[2 * G::BXE], iso, u8_thr));
-            const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(row[3 * G::BXE], iso, u8_thr));
-            if (lane == 0) *reinterpret_cast<uint4*>(&C.rows[buf][4 * warp]) = make_uint4(b0, b1, b2, b3);
-            if (warp == (int)((gl0 + l + 3) & 7)) {
-                const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(layer[32 * G::BXE + lane], iso, u8_thr));
-                const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(layer[lane * G::BXE + 32], iso, u8_thr));
-                const bool corner = below<FT>(layer[32 * G::BXE + 32], iso, u8_thr);
-                if (lane == 0) {
-                    C.rows[buf][32] = r32;
-                    C.col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
-                }
-            }
-        }
+        const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(v[l][0], iso, u8_thr));
+        const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(v[l][1], iso, u8_thr));
+        const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(v[l][2], iso, u8_thr));
+        const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(v[l][3], iso, u8_thr));
+        if (l < nl && lane == 0)
+            *reinterpret_cast<uint4*>(&C.rows[(gl0 + l) & (kRowBuffers - 1)][4 * warp]) = make_uint4(b0, b1, b2, b3);
+    }
+    const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(e_row, iso, u8_thr));
+    const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(e_col, iso, u8_thr));
+    const bool corner = below<FT>(e_corner, iso, u8_thr);
+    if (le < nl && lane == 0) {
+        const uint32_t buf = (gl0 + le) & (kRowBuffers - 1);
+        C.rows[buf][32] = r32;
+        C.col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
     }
 }
 
