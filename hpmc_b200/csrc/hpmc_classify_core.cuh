@@ -57,7 +57,8 @@ __device__ __forceinline__ void write_codes(const Volume& V, uint32_t packed, in
 // for any tiling (tiles narrower than 32 cells), unaligned pitches and
 // functor fields.  Each thread loads its quad's 3x3x2 samples directly; the
 // quads are numbered in Morton order, so thread t's four codes are word t of
-// the block's arena slot.
+// the block's arena slot, and threads 8l .. 8l+7 (one eighth of a warp) hold
+// Morton tile l, whose active mask and vertices they combine by shuffles.
 template <int FT, class UF = NoUserField>
 __device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b, uint8_t* s_cnt,
                                                     uint32_t* s_warp) {
@@ -91,19 +92,34 @@ __device__ __forceinline__ void classify_block_body(const Volume& V, uint64_t b,
             if (V.codes_out) write_codes(V, packed, x, y, z);
         }
     }
-    // thread = quad = cells 4 tid .. 4 tid + 3 in Morton order: its vertices,
-    // one block reduction for the block's count
-    uint32_t vs = 0;
+    // thread = quad = cells 4 tid .. 4 tid + 3 in Morton order: its vertices
+    // and active cells, the tile's by shuffles within its eight lanes, one
+    // block reduction for the block's count
+    uint32_t vs = 0, nib = 0;
 #pragma unroll
-    for (int c = 0; c < 4; c++) vs += s_cnt[(packed >> (8 * c)) & 0xffu];
-    vs = __reduce_add_sync(0xffffffffu, vs);
-    if (lane == 0) s_warp[warp] = vs;
+    for (int c = 0; c < 4; c++) {
+        const uint32_t n = s_cnt[(packed >> (8 * c)) & 0xffu];
+        vs += n;
+        nib |= (n ? 1u : 0u) << c;
+    }
+    uint32_t tmask = nib << (4 * (tid & 7)), tcnt = vs;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        tmask |= __shfl_xor_sync(0xffffffffu, tmask, o);
+        tcnt += __shfl_xor_sync(0xffffffffu, tcnt, o);
+    }
+    const uint32_t wsum = __reduce_add_sync(0xffffffffu, vs);
+    if (lane == 0) s_warp[warp] = wsum;
     __syncthreads();
     uint32_t total = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; w++) total += s_warp[w];
     if (tid == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
-    if (total) V.arena[block_slot(V, b) * kSlotWords + tid] = packed;
+    if (total) {
+        uint32_t* slot = V.arena + block_slot(V, b) * kSlotWords;
+        slot[tid] = packed;
+        if ((tid & 7) == 0) reinterpret_cast<uint2*>(slot + kSlotTileWord)[tid >> 3] = make_uint2(tmask, tcnt);
+    }
     __syncthreads();
 }
 

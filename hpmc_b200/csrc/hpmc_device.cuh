@@ -36,8 +36,11 @@ constexpr int kBlockKeys = 1024;
 constexpr int kMaxLevels = 40;
 
 // Arena slot of a non-empty block: its codes in Morton order, four per word
-// (cell 4i + c in byte c of word i).
-constexpr int kSlotWords = kBlockKeys / 4;
+// (cell 4i + c in byte c of word i), then per Morton tile t of 32 cells
+// (t = 0..31) the pair {active-cell mask (bit i = cell 32t + i), vertices} at
+// words kSlotTileWord + 2t, +1.
+constexpr int kSlotTileWord = kBlockKeys / 4;
+constexpr int kSlotWords = kSlotTileWord + 64;
 constexpr size_t kSlotBytes = sizeof(uint32_t) * (size_t)kSlotWords;
 
 // Active-cell list of one block (a traversal warp's shared memory): one word

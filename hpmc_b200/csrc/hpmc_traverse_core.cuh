@@ -66,27 +66,24 @@ __device__ __forceinline__ uint32_t list_entry(const uint32_t* list, uint32_t j)
 }
 
 // One warp: block b's active-cell list into `list` from its arena slot (1024
-// codes in Morton order, one slot word per quad).  Lane l takes the codes of
-// Morton cells 32l .. 32l+31 (two 16-byte loads) and counts their vertices
-// (32 independent table reads); one warp scan of (cells << 16 | vertices)
-// gives every lane its first list entry and first vertex, and the lane
-// writes its active cells in order.  32 sentinels follow the last entry.
+// codes in Morton order, one slot word per quad, and per Morton tile of 32
+// cells its active mask and vertices).  Lane l takes tile l: its codes (two
+// 16-byte loads) and its mask and vertices (one 8-byte load); one warp scan
+// of (cells << 16 | vertices) gives every lane its first list entry and first
+// vertex, and the lane writes its active cells in order.  32 sentinels follow
+// the last entry.
 __device__ __forceinline__ void load_block(const Volume& V, const uint8_t* s_cnt, uint32_t* list, int lane,
                                            uint32_t b) {
     long long slot = block_slot(V, b);
     slot = slot < V.arena_slots ? slot : V.arena_slots - 1;  // in range for consistent data
-    const uint4* src = reinterpret_cast<const uint4*>(V.arena + slot * kSlotWords) + 2 * lane;
+    const uint32_t* sw = V.arena + slot * kSlotWords;
+    const uint4* src = reinterpret_cast<const uint4*>(sw) + 2 * lane;
     const uint4 w0 = __ldg(src), w1 = __ldg(src + 1);
+    const uint2 tile = __ldg(reinterpret_cast<const uint2*>(sw + kSlotTileWord) + lane);
     const uint32_t w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-    uint32_t vsum = 0, amask = 0;
-#pragma unroll
-    for (int i = 0; i < 32; i++) {
-        const uint32_t c = s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
-        vsum += c;
-        if (c) amask |= 1u << i;
-    }
+    const uint32_t amask = tile.x;
     // block totals < 2^16 each
-    const uint32_t mine = vsum | ((uint32_t)__popc(amask) << 16);
+    const uint32_t mine = (tile.y & 0xffffu) | ((uint32_t)__popc(amask) << 16);
     uint32_t scan = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -351,8 +348,10 @@ __device__ __forceinline__ EdgeGeom edge_of(const TraverseSmem& S, const VertexC
 // ---------------------------------------------------------------------------
 // The extraction: every vertex of the last build (up to the outputs'
 // capacity), in the reference's vertex order.  UF: a caller's functor type
-// when FT == kFieldUser (include/hpmc_functor.cuh).
-template <int FT, int MODE, class UF = NoUserField>
+// when FT == kFieldUser (include/hpmc_functor.cuh).  EXTRA: the interleaved
+// feedback and inspection outputs may be set (false: positions and normals
+// only, without their per-vertex tests).
+template <int FT, int MODE, class UF = NoUserField, bool EXTRA = true>
 __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_constant__ Volume V,
                                                                const __grid_constant__ TraverseOut O) {
     extern __shared__ __align__(16) uint8_t s_traverse[];
@@ -386,14 +385,14 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
             const unsigned long long o = V.vertex_base + v;
             if (O.pos) __stcs(O.pos + o, make_float4(p[0], p[1], p[2], 1.0f));
             if (O.nrm) __stcs(O.nrm + o, make_float4(n[0], n[1], n[2], 0.0f));
-            if (O.feedback) {
+            if (EXTRA && O.feedback) {
                 float2* fb = reinterpret_cast<float2*>(O.feedback + 6ull * o);
                 __stcs(fb + 0, make_float2(n[0], n[1]));
                 __stcs(fb + 1, make_float2(n[2], p[0]));
                 __stcs(fb + 2, make_float2(p[1], p[2]));
             }
-            if (O.dbg_cell) O.dbg_cell[o] = make_int4(c.x, c.y, c.z, c.code | (c.k << 8) | (g.edge << 16));
-            if (O.dbg_t) O.dbg_t[o] = t;
+            if (EXTRA && O.dbg_cell) O.dbg_cell[o] = make_int4(c.x, c.y, c.z, c.code | (c.k << 8) | (g.edge << 16));
+            if (EXTRA && O.dbg_t) O.dbg_t[o] = t;
         }
     }
     finish_queue(V);

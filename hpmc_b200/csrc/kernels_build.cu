@@ -80,6 +80,13 @@ __device__ __forceinline__ void slices_to_codes(const uint32_t c[8], uint32_t w[
     }
 }
 
+// 16 bits -> Morton positions of an 8x2 cell tile: bit x of the low byte goes
+// to bit (x0 | x1 << 2 | x2 << 4), bit x of the high byte to that + 8.
+__device__ __forceinline__ uint32_t spread16(uint32_t t) {
+    t = (t | (t << 12)) & 0x0F0F0F0Fu;
+    return (t | (t << 2)) & 0x33333333u;
+}
+
 // One warp: classify slice z of footprint (fx, fy) from sample-bit rows of the
 // lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Every block
 // gets its level-5 count; blocks with vertices store their codes in Morton
@@ -139,11 +146,13 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
     uint32_t w[8];
     slices_to_codes(c, w);
     if (has_vertices) {
-        // the block's vertices: 32 independent count lookups per lane, one
-        // warp reduction (inactive cells have codes 0 or 255, count 0)
-        uint32_t vs = 0;
+        // the block's vertices: 32 independent count lookups per lane (byte j
+        // of seg = the row's cells 8j .. 8j+7, at most 96), one warp
+        // reduction (inactive cells have codes 0 or 255, count 0)
+        uint32_t seg = 0;
 #pragma unroll
-        for (int i = 0; i < 32; i++) vs += s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu];
+        for (int i = 0; i < 32; i++) seg += (uint32_t)s_cnt[(w[i >> 2] >> (8 * (i & 3))) & 0xffu] << (8 * (i >> 3));
+        const uint32_t vs = (seg & 0xffu) + ((seg >> 8) & 0xffu) + ((seg >> 16) & 0xffu) + (seg >> 24);
         const uint32_t total = __reduce_add_sync(0xffffffffu, vs);
         if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = total;
         // codes in Morton order: word q of the slot = quad (qx, qy), cells
@@ -171,6 +180,22 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
             const uint32_t ispread = (uint32_t)((i & 1) | ((i & 2) << 1) | ((i & 4) << 2));
             dst[qbase | ispread] = word;
         }
+        // Morton tile q = lane (cells 32q .. 32q+31, an 8x4 tile at rows
+        // ty .. ty+3, columns tx .. tx+7; Morton bits x0 y0 x1 y1 x2 | y2 x3
+        // y3 x4 y4): its active mask gathered from four rows in Morton order
+        // and its vertices from the rows' segment counts
+        const uint32_t q = (uint32_t)lane;
+        const int ty = 4 * (int)((q & 1u) | ((q >> 1) & 2u) | ((q >> 2) & 4u));
+        const uint32_t tx = 8u * (((q >> 1) & 1u) | ((q >> 2) & 2u));
+        uint32_t r[4], tcnt = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            r[i] = (__shfl_sync(0xffffffffu, active, ty + i) >> tx) & 0xffu;
+            tcnt += (__shfl_sync(0xffffffffu, seg, ty + i) >> tx) & 0xffu;
+        }
+        // rows 0/2 on Morton bit 3 = 0/1 with bit 1 = 0; rows 1/3 shifted by 2 (bit 1 = 1)
+        const uint32_t tmask = spread16(r[0] | (r[2] << 8)) | (spread16(r[1] | (r[3] << 8)) << 2);
+        reinterpret_cast<uint2*>(dst + kSlotTileWord)[lane] = make_uint2(tmask, tcnt);
     }
     if (V.codes_out) {
         const int y = fy * 32 + lane;

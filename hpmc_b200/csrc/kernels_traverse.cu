@@ -459,13 +459,17 @@ cudaError_t launch_mesh(const Volume& V, const MeshIO& M, int normal_mode, int t
 cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mode, int grid,
                             cudaStream_t st) {
     const int mode = V.binary ? kModeBinary : (normal_mode == kNormalsCentral ? kModeCentral : kModeForward);
-#define HPMC_TRAVERSE_CASE(FT_)                                                                              \
-    case FT_:                                                                                                \
-        if (mode == kModeBinary)                                                                             \
-            return launch_dependent(traverse_kernel<FT_, kModeBinary>, grid, kThreads, kTraverseSmem, st, V, O);  \
-        if (mode == kModeCentral)                                                                            \
-            return launch_dependent(traverse_kernel<FT_, kModeCentral>, grid, kThreads, kTraverseSmem, st, V, O); \
-        return launch_dependent(traverse_kernel<FT_, kModeForward>, grid, kThreads, kTraverseSmem, st, V, O);
+    const bool extra = O.feedback || O.dbg_cell || O.dbg_t;
+#define HPMC_TRAVERSE_LAUNCH(FT_, MODE_)                                                                          \
+    return extra ? launch_dependent(traverse_kernel<FT_, MODE_, NoUserField, true>, grid, kThreads, kTraverseSmem, \
+                                    st, V, O)                                                                     \
+                 : launch_dependent(traverse_kernel<FT_, MODE_, NoUserField, false>, grid, kThreads, kTraverseSmem, \
+                                    st, V, O);
+#define HPMC_TRAVERSE_CASE(FT_)                                             \
+    case FT_:                                                               \
+        if (mode == kModeBinary) HPMC_TRAVERSE_LAUNCH(FT_, kModeBinary)     \
+        if (mode == kModeCentral) HPMC_TRAVERSE_LAUNCH(FT_, kModeCentral)   \
+        HPMC_TRAVERSE_LAUNCH(FT_, kModeForward)
     switch (V.ftype) {
         HPMC_TRAVERSE_CASE(kFieldF32)
         HPMC_TRAVERSE_CASE(kFieldU8)
@@ -475,6 +479,7 @@ cudaError_t launch_traverse(const Volume& V, const TraverseOut& O, int normal_mo
         default: return cudaErrorInvalidValue;
     }
 #undef HPMC_TRAVERSE_CASE
+#undef HPMC_TRAVERSE_LAUNCH
 }
 
 cudaError_t launch_adjoint(const Volume& V, const AdjointIO& A, int normal_mode, int grid, cudaStream_t st) {
