@@ -17,10 +17,13 @@
 //      following 32 level-5 entries (one coalesced load) when it lies there.
 //   2. in-block lookup (warp-cooperative; replaces the base-level steps of
 //      shadergen.cpp:469-495): the classifier left every non-empty block's
-//      active cells (count > 0) with their first vertex, in vertex order, in
-//      the block's arena slot; per round a lane's cell is found from that
-//      list with one OR-reduction of the cell starts that fall in the
-//      round's window and a popcount (no per-vertex search, no recount).
+//      1024 codes in Morton order and, per 32-cell Morton tile, its active
+//      mask and vertex count in the block's arena slot; a warp entering the
+//      block turns them into the block's active-cell list (cells with their
+//      first vertex, in vertex order) in its shared memory with one scan, and
+//      per round a lane's cell is found from that list with one OR-reduction
+//      of the cell starts that fall in the round's window and a popcount (no
+//      per-vertex search).
 //   3. geometry (shadergen.cpp:497-563): edge from the case table, crossing
 //      parameter t, position and normal; FP32 arithmetic with a float-float
 //      fallback for ill-conditioned normals; coalesced streaming float4
