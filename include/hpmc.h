@@ -401,8 +401,8 @@ int HPMCbatchAutotune(struct HPMCBatch* b, float* positions, float* normals, siz
  * the count and the outputs of that call are invalid).  Both are written on
  * the stream after the extraction, so no host sync is needed to read them in
  * stream order.  extent may be NULL (1,1,1).  Work is issued on
- * `cuda_stream`.  Lattices whose pyramid and active-cell lists do not fit
- * the scratch (e.g. larger than about 150^3) are rejected with
+ * `cuda_stream`.  Lattices whose pyramid and block codes do not fit
+ * the scratch (e.g. larger than about 225^3) are rejected with
  * HPMC_ERR_TOO_LARGE.  The first call on a device looks up the scratch
  * array's device address and configures the kernels, so make it before any
  * stream capture.  All calls share the one scratch array, which keeps the
