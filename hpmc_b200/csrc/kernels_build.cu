@@ -240,6 +240,8 @@ static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4
 // Bit rows of the nl layers of one box (stage st), layer l stored at
 // running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
 // row 32 and column x0+32 of layer g go to warp (g + 3) mod 8.
+static_assert(kWarps == 8 && kLayersPerBox <= kWarps, "a box's layers and slices map onto the 8 warps mod 8");
+
 template <int FT>
 __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st, int nl, uint32_t gl0, float iso,
                                             int u8_thr, int warp, int lane, ColumnSmem& C) {
@@ -257,7 +259,7 @@ __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st
 #pragma unroll
         for (int i = 0; i < 4; i++) v[l][i] = row[l * G::LAYER + i * G::BXE];
     const int le = (int)(((uint32_t)warp - gl0 - 3u) & 7u);  // the layer whose row 32 and column 32 this warp takes
-    const T* layer = st + le * G::LAYER;
+    const T* layer = st + (le < kLayersPerBox ? le : 0) * G::LAYER;  // inside the stage for any box depth
     const T e_row = layer[32 * G::BXE + lane], e_col = layer[lane * G::BXE + 32], e_corner = layer[32 * G::BXE + 32];
 #pragma unroll
     for (int l = 0; l < kLayersPerBox; l++) {
