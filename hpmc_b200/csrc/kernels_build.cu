@@ -338,11 +338,12 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
     __syncthreads();
     // test hook: the first column of the volume never receives box stall_box
     const int stall = (fx == 0 && fy == 0 && zc == 0) ? V.stall_box : -1;
+    const uint64_t pol = l2_evict_first_policy();  // the field is read once
     if (tid == 0) {
         for (int k = 0; k < kRingStages && k < nbox; k++) {
             if (k == stall) continue;
             mbar_arrive_expect_tx(&C.bar[k], G::STAGE_BYTES);
-            tma_load_3d(s_ring + k * G::STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &C.bar[k]);
+            tma_load_3d(s_ring + k * G::STAGE_STRIDE, tmap, x0, y0, z0 + k * kLayersPerBox, &C.bar[k], pol);
         }
     }
     const uint32_t vmask = row_mask(V, x0, y0, lane);
@@ -366,7 +367,7 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
         if (tid == 0 && k + kRingStages < nbox && k + kRingStages != stall) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
             tma_load_3d(s_ring + s * G::STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox,
-                        &C.bar[s]);
+                        &C.bar[s], pol);
         }
         classify_box_slices(V, z0, fx, fy, lb, nl, 0u, warp, lane, vmask, full, C);
     }
@@ -427,6 +428,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     // following column is claimed one column ahead (pnext), so the atomic's
     // round trip overlaps the current column
     int pu = -1, pk = 0, pnl = 0, pz0 = 0, pfx = 0, pfy = 0, pnext = -1;
+    const uint64_t pol = l2_evict_first_policy();  // the field is read once
     bool pdone = false;
     uint32_t issued = 0;
     if (tid == 0) pnext = (int)atomicAdd(&V.ctrl->col_next, 1u);
@@ -450,7 +452,8 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         // test hook: a CTA never issues its box stall_box (its waits run out)
         if ((int)issued != V.stall_box) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
-            tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, pfx * 32, pfy * 32, pz0 + pk * kLayersPerBox, &C.bar[s]);
+            tma_load_3d(s_ring + s * G::STAGE_STRIDE, &tmap, pfx * 32, pfy * 32, pz0 + pk * kLayersPerBox, &C.bar[s],
+                        pol);
         }
         issued++;
         pk++;
