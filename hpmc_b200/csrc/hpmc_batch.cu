@@ -7,7 +7,7 @@
 // Device memory of a batch (one allocation):
 //   batch control block | per-volume control blocks | descriptors |
 //   tensor maps | brick, reduce-chunk and work-item prefix arrays |
-//   output offsets | dense levels of every volume | active-cell list arenas
+//   output offsets | dense levels of every volume | block-code arenas
 #include <cuda.h>
 #include <cuda_runtime.h>
 

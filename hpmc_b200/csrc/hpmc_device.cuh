@@ -76,7 +76,6 @@ enum NormalMode : int {
 // Device control block of one pyramid (one volume).
 struct Ctrl {
     unsigned long long total;    // vertex count (top of the pyramid)
-    unsigned int arena_used;     // arena slots handed out by the current build
     unsigned int reduce_done;    // last-block-done counter of the reduce kernel
     unsigned int status;         // sticky error bits (kStatus*)
     unsigned int written;        // vertices written by the last extraction
@@ -84,13 +83,12 @@ struct Ctrl {
     unsigned int work_done;      // traversal CTAs finished (the last one resets the queue)
     unsigned int col_next;       // column classifier's work queue: next column to claim
     unsigned int col_done;       // column classifier CTAs finished (the last one resets the queue)
-    unsigned int pad[3];
+    unsigned int pad[4];
 };
 
 enum : unsigned int {
     kStatusOverflow = 1u,      // vertex count does not fit the level type
     kStatusCapacity = 2u,      // output buffer smaller than the vertex count
-    kStatusArena = 4u,         // arena overflow (never expected: sized for all blocks)
     kStatusTimeout = 8u,       // a bounded wait gave up
 };
 
