@@ -249,7 +249,7 @@ int HPMCreadLevel(struct HPMCHistoPyramid* h, int level, uint32_t* host_out, siz
 int HPMCsetTraversalDebugBuffers(struct HPMCTraversalHandle* th, int32_t* cell_info, float* t);
 
 /* Device status word of the pyramid (bits: 1 overflow, 2 capacity,
- * 4 arena, 8 timeout); waits for the handle's stream. */
+ * 8 timeout); waits for the handle's stream. */
 int HPMCgetDeviceStatus(struct HPMCHistoPyramid* h, unsigned int* status);
 
 /* Test hook for failure detection (no counterpart in the reference; it
