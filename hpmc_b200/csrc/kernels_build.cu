@@ -91,8 +91,9 @@ __device__ __forceinline__ uint32_t spread16(uint32_t t) {
 // lower layer (rows_b/col_b) and the upper layer (rows_t/col_t).  Every block
 // gets its level-5 count; blocks with vertices store their codes in Morton
 // order in their slot.  full: every cell of the footprint lies inside the
-// grid (vmask is all ones in every lane).
-__device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, int lane,
+// grid (vmask is all ones in every lane).  b: the block's level-5 index,
+// column_block_index(V, z, fx, fy).
+__device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int fx, int fy, uint32_t b, int lane,
                                                     uint32_t vmask, bool full, const uint32_t* rows_b,
                                                     uint64_t col_b, const uint32_t* rows_t, uint64_t col_t,
                                                     const uint8_t* s_cnt) {
@@ -112,7 +113,7 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
         const bool below_all = ((a0 & a1 & b0 & b1) == 0xffffffffu) && ((cb & ct) == 3u);
         const bool above_all = ((a0 | a1 | b0 | b1) == 0u) && ((cb | ct) == 0u);
         if (__all_sync(0xffffffffu, below_all) || __all_sync(0xffffffffu, above_all)) {
-            if (lane == 0) V.levels[V.level_off[kBlockLevel] + column_block_index(V, z, fx, fy)] = 0u;
+            if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = 0u;
             return;
         }
     }
@@ -135,7 +136,6 @@ __device__ __forceinline__ void classify_slice_warp(const Volume& V, int z, int 
     // vertices (every other MC case has at least one triangle)
     const uint32_t active = (all ^ any) & vmask;
     const bool has_vertices = __any_sync(0xffffffffu, active != 0u);
-    const uint64_t b = column_block_index(V, z, fx, fy);
     if (!has_vertices) {
         if (lane == 0) V.levels[V.level_off[kBlockLevel] + b] = 0u;
         if (!V.codes_out) return;
@@ -234,7 +234,12 @@ struct ColumnSmem {
     uint64_t col[kRowBuffers];                   // bit r = sample (x0 + 32, y0 + r) below iso; bit 32 = corner
     uint64_t bar[kRingStages];
     uint8_t cnt[256];
+    // level-5 index of block (0, 0) of slice z, z < kSliceTable: a footprint's
+    // block is that OR its own Morton part (the footprint's bits lie below
+    // the tile's), so a slice costs one load instead of two bit spreads
+    uint32_t zbase[1024];
 };
+constexpr int kSliceTable = 1024;
 static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4 row stores need 16-byte alignment");
 
 // Bit rows of the nl layers of one box (stage st), layer l stored at
@@ -280,19 +285,35 @@ __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st
     }
 }
 
+// Morton part of footprint (fx, fy) in a block index.
+__device__ __forceinline__ uint32_t footprint_morton(int fx, int fy) {
+    return morton_spread16((uint32_t)fx) | (morton_spread16((uint32_t)fy) << 1);
+}
+
+// The slice table for slices 0 .. min(cells, kSliceTable)-1 (all threads).
+__device__ __forceinline__ void fill_slice_table(const Volume& V, ColumnSmem& C) {
+    const int n = min(V.cells[2], kSliceTable);
+    for (int z = threadIdx.x; z < n; z += blockDim.x) C.zbase[z] = (uint32_t)column_block_index(V, z, 0, 0);
+}
+
+__device__ __forceinline__ uint32_t slice_block(const Volume& V, const ColumnSmem& C, int z, uint32_t fm) {
+    return (z < kSliceTable ? C.zbase[z] : (uint32_t)column_block_index(V, z, 0, 0)) | fm;
+}
+
 // After the box barrier: the slices whose upper layer arrived in this box
 // (column-relative slices lb-1 .. lb+nl-2), warp (glu + slice) mod 8 each, so
 // the work rotates over the warps from box to box.  glu = running index of
 // the column's layer 0.
-__device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, int lb, int nl,
-                                                    uint32_t glu, int warp, int lane, uint32_t vmask, bool full,
-                                                    ColumnSmem& C) {
+__device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, uint32_t fm, int lb,
+                                                    int nl, uint32_t glu, int warp, int lane, uint32_t vmask,
+                                                    bool full, ColumnSmem& C) {
     // the slice of this warp, if any
     const int sl = lb - 1 + (int)(((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u);
     if (sl >= 0 && sl <= lb + nl - 2) {
         const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
-        classify_slice_warp(V, z0 + sl, fx, fy, lane, vmask, full, C.rows[bb], C.col[bb], C.rows[bt], C.col[bt],
-                            C.cnt);
+        const int z = z0 + sl;
+        classify_slice_warp(V, z, fx, fy, slice_block(V, C, z, fm), lane, vmask, full, C.rows[bb], C.col[bb],
+                            C.rows[bt], C.col[bt], C.cnt);
     }
 }
 
@@ -331,6 +352,8 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
     const int u8_thr = V.u8_thr;
 
     C.cnt[tid] = c_vertex_count[tid];
+    fill_slice_table(V, C);
+    const uint32_t fm = footprint_morton(fx, fy);
     if (tid == 0) {
         for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
         mbar_fence_init();
@@ -369,7 +392,7 @@ __device__ __forceinline__ void classify_column_body(const CUtensorMap* tmap, co
             tma_load_3d(s_ring + s * G::STAGE_STRIDE, tmap, x0, y0, z0 + (k + kRingStages) * kLayersPerBox,
                         &C.bar[s], pol);
         }
-        classify_box_slices(V, z0, fx, fy, lb, nl, 0u, warp, lane, vmask, full, C);
+        classify_box_slices(V, z0, fx, fy, fm, lb, nl, 0u, warp, lane, vmask, full, C);
     }
     if (timed_out) {
         // drain the boxes still in flight (bounded) before the CTA exits
@@ -397,8 +420,9 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     uint8_t* const s_ring = ring_base<FT>();
     __shared__ __align__(16) ColumnSmem C;
     // per ring stage: box k | layers << 16 of its column (-1: end), footprint
-    // (fx, fy) and first slice -- decoded once by the producer, so that the
-    // consumers start converting without integer divisions after each wait
+    // fx | fy << 16, first slice and the footprint's Morton part -- decoded
+    // once by the producer, so that the consumers start converting without
+    // integer divisions after each wait
     __shared__ int4 s_tag[kRingStages];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int per_slab = V.nfx * V.nfy;
@@ -415,6 +439,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     };
 
     C.cnt[tid] = c_vertex_count[tid];
+    fill_slice_table(V, C);
     if (tid == 0) {
         for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
         mbar_fence_init();
@@ -448,7 +473,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             }
             column(pu, pfx, pfy, pz0, pnl);
         }
-        s_tag[s] = make_int4(pk | (pnl << 16), pfx, pfy, pz0);
+        s_tag[s] = make_int4(pk | (pnl << 16), pfx | (pfy << 16), pz0, (int)footprint_morton(pfx, pfy));
         // test hook: a CTA never issues its box stall_box (its waits run out)
         if ((int)issued != V.stall_box) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
@@ -469,7 +494,8 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
         // the stage's tag was written before the producer's arrival (release) on its barrier
         const int4 tag = ok ? s_tag[s] : make_int4(-1, 0, 0, 0);
-        const int fx = tag.y, fy = tag.z, z0 = tag.w;
+        const int fx = tag.y & 0xffff, fy = tag.y >> 16, z0 = tag.z;
+        const uint32_t fm = (uint32_t)tag.w;
         const int k = tag.x & 0xffff, nlayers = tag.x >> 16;
         const int lb = k * kLayersPerBox;
         const int nl = min(kLayersPerBox, nlayers - lb);
@@ -486,7 +512,8 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         if (tid == 0) issue_next();  // refill stage s
         const uint32_t vmask = row_mask(V, fx * 32, fy * 32, lane);
         const bool full = __all_sync(0xffffffffu, vmask == 0xffffffffu);
-        classify_box_slices(V, z0, fx, fy, lb, nl, (pos - (uint32_t)k) * kLayersPerBox, warp, lane, vmask, full, C);
+        classify_box_slices(V, z0, fx, fy, fm, lb, nl, (pos - (uint32_t)k) * kLayersPerBox, warp, lane, vmask, full,
+                            C);
     }
     if (timed_out && tid == 0) {
         // drain the boxes still in flight (bounded) before the CTA exits
