@@ -246,6 +246,7 @@ static_assert(offsetof(ColumnSmem, rows) % 16 == 0 && (36 * 4) % 16 == 0, "uint4
 // running index gl0 + l.  Warp w converts rows 4w .. 4w+3 of every layer;
 // row 32 and column x0+32 of layer g go to warp (g + 3) mod 8.
 static_assert(kWarps == 8 && kLayersPerBox <= kWarps, "a box's layers and slices map onto the 8 warps mod 8");
+static_assert(kRowBuffers % kLayersPerBox == 0, "a box's bit-row buffers never wrap");
 
 template <int FT>
 __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st, int nl, uint32_t gl0, float iso,
@@ -266,20 +267,23 @@ __device__ __forceinline__ void convert_box(const typename ColumnGeom<FT>::T* st
     const int le = (int)(((uint32_t)warp - gl0 - 3u) & 7u);  // the layer whose row 32 and column 32 this warp takes
     const T* layer = st + (le < kLayersPerBox ? le : 0) * G::LAYER;  // inside the stage for any box depth
     const T e_row = layer[32 * G::BXE + lane], e_col = layer[lane * G::BXE + 32], e_corner = layer[32 * G::BXE + 32];
+    // gl0 is a multiple of kLayersPerBox and kRowBuffers of that, so a box's
+    // buffers are g0 .. g0 + kLayersPerBox - 1 without wrapping
+    const uint32_t g0 = gl0 & (kRowBuffers - 1);
+    uint4* const rows_w = reinterpret_cast<uint4*>(&C.rows[g0][4 * warp]);
 #pragma unroll
     for (int l = 0; l < kLayersPerBox; l++) {
         const uint32_t b0 = __ballot_sync(0xffffffffu, below<FT>(v[l][0], iso, u8_thr));
         const uint32_t b1 = __ballot_sync(0xffffffffu, below<FT>(v[l][1], iso, u8_thr));
         const uint32_t b2 = __ballot_sync(0xffffffffu, below<FT>(v[l][2], iso, u8_thr));
         const uint32_t b3 = __ballot_sync(0xffffffffu, below<FT>(v[l][3], iso, u8_thr));
-        if (l < nl && lane == 0)
-            *reinterpret_cast<uint4*>(&C.rows[(gl0 + l) & (kRowBuffers - 1)][4 * warp]) = make_uint4(b0, b1, b2, b3);
+        if (l < nl && lane == 0) rows_w[l * (36 / 4)] = make_uint4(b0, b1, b2, b3);
     }
     const uint32_t r32 = __ballot_sync(0xffffffffu, below<FT>(e_row, iso, u8_thr));
     const uint32_t col = __ballot_sync(0xffffffffu, below<FT>(e_col, iso, u8_thr));
     const bool corner = below<FT>(e_corner, iso, u8_thr);
     if (le < nl && lane == 0) {
-        const uint32_t buf = (gl0 + le) & (kRowBuffers - 1);
+        const uint32_t buf = g0 + (uint32_t)le;
         C.rows[buf][32] = r32;
         C.col[buf] = (uint64_t)col | ((uint64_t)corner << 32);
     }
@@ -424,6 +428,9 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
     // once by the producer, so that the consumers start converting without
     // integer divisions after each wait
     __shared__ int4 s_tag[kRingStages];
+    // per ring stage: the column's x mask and valid rows (bit 31: every row
+    // valid and the mask full), so a lane's row mask is one compare
+    __shared__ uint2 s_rowmask[kRingStages];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int per_slab = V.nfx * V.nfy;
     const float iso = V.binary ? 0.5f : V.iso;
@@ -474,6 +481,12 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             column(pu, pfx, pfy, pz0, pnl);
         }
         s_tag[s] = make_int4(pk | (pnl << 16), pfx | (pfy << 16), pz0, (int)footprint_morton(pfx, pfy));
+        {
+            const int xv = V.cells[0] - pfx * 32, yv = V.cells[1] - pfy * 32;
+            const uint32_t xm = xv >= 32 ? 0xffffffffu : ((1u << xv) - 1u);
+            const uint32_t rows = (uint32_t)min(yv, 32);
+            s_rowmask[s] = make_uint2(xm, rows | ((xm == 0xffffffffu && rows == 32u) ? 0x80000000u : 0u));
+        }
         // test hook: a CTA never issues its box stall_box (its waits run out)
         if ((int)issued != V.stall_box) {
             mbar_arrive_expect_tx(&C.bar[s], G::STAGE_BYTES);
@@ -494,6 +507,7 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         const bool ok = mbar_wait_bounded(&C.bar[s], parity, V.wait_limit_ns, &V.ctrl->status, kStatusTimeout);
         // the stage's tag was written before the producer's arrival (release) on its barrier
         const int4 tag = ok ? s_tag[s] : make_int4(-1, 0, 0, 0);
+        const uint2 rm = ok ? s_rowmask[s] : make_uint2(0u, 0u);  // read before the producer refills stage s
         const int fx = tag.y & 0xffff, fy = tag.y >> 16, z0 = tag.z;
         const uint32_t fm = (uint32_t)tag.w;
         const int k = tag.x & 0xffff, nlayers = tag.x >> 16;
@@ -510,8 +524,8 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         }
         if (tag.x < 0) break;        // the end tag (the same for every thread)
         if (tid == 0) issue_next();  // refill stage s
-        const uint32_t vmask = row_mask(V, fx * 32, fy * 32, lane);
-        const bool full = __all_sync(0xffffffffu, vmask == 0xffffffffu);
+        const uint32_t vmask = (uint32_t)lane < (rm.y & 0xffu) ? rm.x : 0u;  // == row_mask(V, 32 fx, 32 fy, lane)
+        const bool full = (rm.y >> 31) != 0u;
         classify_box_slices(V, z0, fx, fy, fm, lb, nl, (pos - (uint32_t)k) * kLayersPerBox, warp, lane, vmask, full,
                             C);
     }
