@@ -311,10 +311,15 @@ __device__ __forceinline__ uint32_t slice_block(const Volume& V, const ColumnSme
 __device__ __forceinline__ void classify_box_slices(const Volume& V, int z0, int fx, int fy, uint32_t fm, int lb,
                                                     int nl, uint32_t glu, int warp, int lane, uint32_t vmask,
                                                     bool full, ColumnSmem& C) {
-    // the slice of this warp, if any
-    const int sl = lb - 1 + (int)(((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u);
+    // the slice of this warp, if any.  glu + lb is the running index of the
+    // box's first layer, a multiple of kLayersPerBox: with 8-layer boxes the
+    // warp's offset in the box is the same in every box
+    const uint32_t w1 = kLayersPerBox == 8 ? (uint32_t)(warp + 1) & 7u
+                                           : ((uint32_t)warp - (glu + (uint32_t)lb - 1u)) & 7u;
+    const int sl = lb - 1 + (int)w1;
     if (sl >= 0 && sl <= lb + nl - 2) {
-        const uint32_t bb = (glu + sl) & (kRowBuffers - 1), bt = (glu + sl + 1) & (kRowBuffers - 1);
+        const uint32_t g = glu + (uint32_t)sl;
+        const uint32_t bb = g & (kRowBuffers - 1), bt = (g + 1u) & (kRowBuffers - 1);
         const int z = z0 + sl;
         classify_slice_warp(V, z, fx, fy, slice_block(V, C, z, fm), lane, vmask, full, C.rows[bb], C.col[bb],
                             C.rows[bt], C.col[bt], C.cnt);
