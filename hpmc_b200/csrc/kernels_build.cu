@@ -554,17 +554,16 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
 
 // ---------------------------------------------------------------------------
 // Upper reductions (shadergen.cpp:174-225 without the floor filter): level
-// j+1 entry e = sum of level j entries 4e..4e+3.  CTA c reduces 4096 entries
-// of level j_in in shared memory (6 levels); the last CTA to finish carries
-// on from those partial tops to level j_stop.  The top entry is the vertex
-// count (hpiface.cpp:323-327).
+// j+1 entry e = sum of level j entries 4e..4e+3.  CTA c reduces 1024 entries
+// of level j_in (5 levels: registers, shuffles and one shared-memory
+// exchange); the last CTA to finish carries on from those partial tops to
+// level j_stop.  The top entry is the vertex count (hpiface.cpp:323-327).
+// Level-5 entries of padding blocks (footprints past the grid) are zero: the
+// levels are cleared when they are set up and only the generic classifier
+// writes those entries, with zero.
 constexpr int kReduceChunk = 1024;  // level entries per CTA (5 levels)
 constexpr int kReduceTop = 4096;    // entries the last CTA can finish (6 levels)
 
-__device__ __forceinline__ bool level5_valid(const Volume& V, uint64_t b) {
-    int z, fx, fy;
-    return column_block(V, b, z, fx, fy);
-}
 
 __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int& j, int j_stop, long long n,
                             long long out_base, bool& overflow) {
@@ -596,28 +595,52 @@ __device__ void reduce_tree(const Volume& V, uint32_t* buf0, uint32_t* buf1, int
 
 // One chunk of kReduceChunk level-j_in entries (chunk `chunk` of `nchunks`).
 // Returns true in the CTA that wrote the vertex count (level jtop reached).
-__device__ __forceinline__ bool reduce_chunk(const Volume& V, int j_in, int j_stop, int mask_level5,
-                                             long long chunk, unsigned int nchunks, uint32_t* buf0, uint32_t* buf1,
+__device__ __forceinline__ bool reduce_chunk(const Volume& V, int j_in, int j_stop, long long chunk, unsigned int nchunks, uint32_t* buf0, uint32_t* buf1,
                                              int* s_last) {
     bool overflow = false;
     const long long n_in = level_entries(V.size_l2, j_in);
     const long long base = chunk * kReduceChunk;
     const long long n = min((long long)kReduceChunk, n_in - base);  // a power of 4 (>= 4), or 1 at the top
     const int t = threadIdx.x;
-    if (4 * t < n) {
-        uint4 v = *reinterpret_cast<const uint4*>(V.levels + V.level_off[j_in] + base + 4 * t);
-        if (mask_level5) {  // level-5 entries of padding blocks are never written
-            const uint64_t e = (uint64_t)(base + 4 * t);
-            if (!level5_valid(V, e)) v.x = 0;
-            if (!level5_valid(V, e + 1)) v.y = 0;
-            if (!level5_valid(V, e + 2)) v.z = 0;
-            if (!level5_valid(V, e + 3)) v.w = 0;
-        }
-        *reinterpret_cast<uint4*>(&buf0[4 * t]) = v;
-    }
-    __syncthreads();
     int j = j_in;
-    reduce_tree(V, buf0, buf1, j, j_stop, n, base, overflow);
+    if (n == kReduceChunk && j_stop - j_in >= 5) {
+        // a full chunk, five levels without shared-memory round trips: thread
+        // t's four entries make level j+1 entry t, groups of 4 and 16 lanes
+        // (shuffles) levels j+2 and j+3, pairs of warps and then all eight
+        // (one exchange) levels j+4 and j+5.  A chunk's sums stay below 2^32
+        // (1024 entries of at most 15 * 1024 vertices each).
+        const uint4 v = *reinterpret_cast<const uint4*>(V.levels + V.level_off[j_in] + base + 4 * t);
+        uint32_t a = v.x + v.y + v.z + v.w;
+        V.levels[V.level_off[j_in + 1] + (base >> 2) + t] = a;
+        a += __shfl_xor_sync(0xffffffffu, a, 1);
+        a += __shfl_xor_sync(0xffffffffu, a, 2);
+        if ((t & 3) == 0) V.levels[V.level_off[j_in + 2] + (base >> 4) + (t >> 2)] = a;
+        a += __shfl_xor_sync(0xffffffffu, a, 4);
+        a += __shfl_xor_sync(0xffffffffu, a, 8);
+        if ((t & 15) == 0) V.levels[V.level_off[j_in + 3] + (base >> 6) + (t >> 4)] = a;
+        a += __shfl_xor_sync(0xffffffffu, a, 16);
+        if ((t & 31) == 0) buf1[t >> 5] = a;  // the warps' sums
+        __syncthreads();
+        if (t < kWarps / 2) {
+            const uint32_t p = buf1[2 * t] + buf1[2 * t + 1];
+            V.levels[V.level_off[j_in + 4] + (base >> 8) + t] = p;
+            buf1[kWarps + t] = p;
+        }
+        __syncthreads();
+        if (t == 0) {
+            const uint32_t c = buf1[kWarps] + buf1[kWarps + 1] + buf1[kWarps + 2] + buf1[kWarps + 3];
+            V.levels[V.level_off[j_in + 5] + (base >> 10)] = c;
+            buf0[0] = c;
+        }
+        __syncthreads();
+        j = j_in + 5;
+    } else {
+        if (4 * t < n)
+            *reinterpret_cast<uint4*>(&buf0[4 * t]) =
+                *reinterpret_cast<const uint4*>(V.levels + V.level_off[j_in] + base + 4 * t);
+        __syncthreads();
+        reduce_tree(V, buf0, buf1, j, j_stop, n, base, overflow);
+    }
     if (j < j_stop) {
         // levels remain above this chunk's top: the last CTA to finish continues
         __threadfence();
@@ -639,14 +662,13 @@ __device__ __forceinline__ bool reduce_chunk(const Volume& V, int j_in, int j_st
     return j == V.jtop;
 }
 
-__global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant__ Volume V, int j_in, int j_stop,
-                                                          int mask_level5) {
+__global__ void __launch_bounds__(kThreads) reduce_levels(const __grid_constant__ Volume V, int j_in, int j_stop) {
     __shared__ __align__(16) uint32_t buf0[kReduceTop];
     __shared__ uint32_t buf1[kReduceTop / 4];
     __shared__ int s_last;
     wait_prior_grid();
     allow_next_grid();
-    reduce_chunk(V, j_in, j_stop, mask_level5, blockIdx.x, gridDim.x, buf0, buf1, &s_last);
+    reduce_chunk(V, j_in, j_stop, blockIdx.x, gridDim.x, buf0, buf1, &s_last);
 }
 
 // Top entry when the whole pyramid is one block (no reduction launch needed).
@@ -756,8 +778,8 @@ __global__ void __launch_bounds__(kThreads) reduce_batch(const __grid_constant__
     const uint32_t c0 = __ldg(B.reduce_start + v);
     const uint32_t nchunks = __ldg(B.reduce_start + v + 1) - c0;
     // every batch volume reaches its top in this launch (jtop - 5 <= 11)
-    const bool finished = reduce_chunk(sV, kBlockLevel, sV.jtop, sV.column_layout, (long long)(blockIdx.x - c0),
-                                       nchunks, buf0, buf1, &s_last);
+    const bool finished =
+        reduce_chunk(sV, kBlockLevel, sV.jtop, (long long)(blockIdx.x - c0), nchunks, buf0, buf1, &s_last);
     if (!finished) return;  // uniform across the CTA
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -826,8 +848,7 @@ cudaError_t launch_reduce(const Volume& V, cudaStream_t st) {
         const int j_stop = (V.jtop - j_in <= 11) ? V.jtop : j_in + 5;
         const long long n_in = level_entries(V.size_l2, j_in);
         const long long grid = (n_in + kReduceChunk - 1) / kReduceChunk;
-        cudaError_t e = launch_dependent(reduce_levels, (unsigned)grid, kThreads, 0, st, V, j_in, j_stop,
-                                         (j_in == kBlockLevel && V.column_layout) ? 1 : 0);
+        cudaError_t e = launch_dependent(reduce_levels, (unsigned)grid, kThreads, 0, st, V, j_in, j_stop);
         if (e != cudaSuccess) return e;
         j_in = j_stop;
     }
