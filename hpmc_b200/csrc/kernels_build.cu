@@ -24,10 +24,12 @@
 namespace hpmc {
 
 // ---------------------------------------------------------------------------
-// Column classification: CTA = one 32x32 cell footprint of the slice tiles,
-// streaming column_slices slices through a TMA ring of 4-layer sample boxes (each
-// sample leaves HBM once; halo rows/columns are shared with neighbouring
-// CTAs through L2).
+// Column classification: a column = one 32x32 cell footprint of the slice
+// tiles x column_slices slices, streamed through a TMA ring of 8-layer
+// sample boxes (each sample leaves HBM once; halo rows/columns are shared
+// with neighbouring columns through L2).  The single-volume kernel is
+// persistent (columns from a device queue); the batched one takes one column
+// brick per CTA.
 //
 // Per layer, every warp turns rows of samples into bits (f < iso) with one
 // ballot per row.  Per slice, ONE warp classifies the whole 32x32 block,
@@ -36,8 +38,9 @@ namespace hpmc {
 // marks the cells that are neither all-inside nor all-outside (the only ones
 // with vertices); only those go through the count table.  The warp sum is the
 // block's level-5 entry; non-empty blocks also store their 1024 codes in
-// Morton order in their arena slot (1 KiB), from which a traversal warp
-// builds the block's active-cell list when it enters the block.
+// Morton order and each 32-cell tile's active mask and vertex count in their
+// arena slot (1.25 KiB), from which a traversal warp builds the block's
+// active-cell list when it enters the block.
 //
 // Measured alternatives for the list: written by the classifier (each
 // non-empty block's serial gathers stall the box barrier: +20 us at 512^3),
