@@ -79,11 +79,25 @@ struct HPMCHistoPyramid {
     int layout[6] = {0, 0, 0, 0, 0, 0};
     // device state
     Volume V{};
-    uint32_t* d_levels = nullptr;
-    size_t levels_cap = 0;  // entries
-    uint32_t* d_arena = nullptr;
-    size_t arena_cap = 0;   // slots
+    // Column layouts keep two sets of levels and arena, and builds alternate
+    // between them: a build may then overlap the previous extraction, which
+    // reads the other set (Volume::overlap).  One control block.
+    uint32_t* d_levels = nullptr;  // nsets x levels_cap entries
+    size_t levels_cap = 0;         // entries per set
+    uint32_t* d_arena = nullptr;   // nsets x arena_cap slots
+    size_t arena_cap = 0;          // slots per set
+    int nsets = 0;
+    int set = 0;                   // the set of the last build
     Ctrl* d_ctrl = nullptr;
+    // the last extraction's outputs (byte ranges) and stream: the next build
+    // overlaps it only on the same stream and with a field that is none of them
+    struct Range {
+        const void* p;
+        size_t n;
+    };
+    Range last_out[5] = {};
+    cudaStream_t last_out_stream = nullptr;
+    bool have_last_out = false;
     uint8_t* codes_capture = nullptr;
     CUtensorMap tmap;
     bool have_tmap = false;
@@ -129,6 +143,7 @@ void release_device(HPMCHistoPyramid* h) {
     h->d_arena = nullptr;
     h->d_ctrl = nullptr;
     h->levels_cap = h->arena_cap = 0;
+    h->nsets = 0;
 }
 
 // Resolve the field source into the Volume's field members.
@@ -185,16 +200,17 @@ bool setup(HPMCHistoPyramid* h) {
     long long levels_total = 0, slots = 0;
     hpmc::host::volume_layout(V, h->lattice, h->cells, h->extent, L, &levels_total, &slots);
     V.column_slices = hpmc::host::default_column_slices(V, h->constants->num_sms);
+    const int nsets = V.column_layout ? 2 : 1;
     // (re)allocate
-    if ((size_t)levels_total > h->levels_cap || (size_t)slots > h->arena_cap || !h->d_ctrl) {
+    if ((size_t)levels_total > h->levels_cap || (size_t)slots > h->arena_cap || nsets > h->nsets || !h->d_ctrl) {
         if (h->d_ctrl && cudaStreamSynchronize(h->stream) != cudaSuccess) {
             cudaGetLastError();
             h->status = HPMC_ERR_CUDA;
             return false;
         }
         release_device(h);
-        if (cudaMalloc(&h->d_levels, sizeof(uint32_t) * levels_total) != cudaSuccess ||
-            cudaMalloc(&h->d_arena, hpmc::kSlotBytes * (size_t)slots) != cudaSuccess ||
+        if (cudaMalloc(&h->d_levels, sizeof(uint32_t) * levels_total * nsets) != cudaSuccess ||
+            cudaMalloc(&h->d_arena, hpmc::kSlotBytes * (size_t)slots * nsets) != cudaSuccess ||
             cudaMalloc(&h->d_ctrl, sizeof(Ctrl)) != cudaSuccess) {
             cudaGetLastError();
             release_device(h);
@@ -203,9 +219,11 @@ bool setup(HPMCHistoPyramid* h) {
         }
         h->levels_cap = (size_t)levels_total;
         h->arena_cap = (size_t)slots;
+        h->nsets = nsets;
     }
+    // every set's levels start at zero (padding blocks' level-5 entries stay zero)
     if (cudaMemsetAsync(h->d_ctrl, 0, sizeof(Ctrl), h->stream) != cudaSuccess ||
-        cudaMemsetAsync(h->d_levels, 0, sizeof(uint32_t) * levels_total, h->stream) != cudaSuccess) {
+        cudaMemsetAsync(h->d_levels, 0, sizeof(uint32_t) * h->levels_cap * h->nsets, h->stream) != cudaSuccess) {
         cudaGetLastError();
         h->status = HPMC_ERR_CUDA;
         return false;
@@ -214,6 +232,7 @@ bool setup(HPMCHistoPyramid* h) {
     V.arena = h->d_arena;
     V.arena_slots = slots;
     V.ctrl = h->d_ctrl;
+    h->set = 0;
     h->tainted = false;
     h->built = false;
     h->count_valid = false;
@@ -258,7 +277,33 @@ int launch_extract(HPMCTraversalHandle* th, float* pos, float* nrm, float* feedb
         set_error(h, HPMC_ERR_CUDA, true);
         return HPMC_ERR_CUDA;
     }
+    h->last_out[0] = {O.pos, O.pos ? cap * sizeof(float4) : 0};
+    h->last_out[1] = {O.nrm, O.nrm ? cap * sizeof(float4) : 0};
+    h->last_out[2] = {O.feedback, O.feedback ? cap * 6 * sizeof(float) : 0};
+    h->last_out[3] = {O.dbg_cell, O.dbg_cell ? cap * sizeof(int4) : 0};
+    h->last_out[4] = {O.dbg_t, O.dbg_t ? cap * sizeof(float) : 0};
+    h->last_out_stream = h->stream;
+    h->have_last_out = true;
     return (h->count_valid && h->count_cached > cap) ? HPMC_ERR_CAPACITY : HPMC_OK;
+}
+
+// A build may overlap the previous extraction (Volume::overlap) when it
+// runs the column classifier on the extraction's stream, captures no codes,
+// and its field bytes are none of the extraction's outputs.
+bool may_overlap_extraction(const HPMCHistoPyramid* h) {
+    if (!h->V.column_layout || !h->have_tmap || h->nsets < 2 || h->codes_capture || !h->have_last_out ||
+        h->last_out_stream != h->stream || h->fmode != HPMCHistoPyramid::kArray)
+        return false;
+    const FieldDesc& f = h->field;
+    const size_t es = elem_size(f.type);
+    const size_t rp = f.row_pitch ? f.row_pitch : (size_t)h->lattice[0] * es;
+    const size_t sp = f.slice_pitch ? f.slice_pitch : rp * (size_t)h->lattice[1];
+    const uintptr_t a = (uintptr_t)f.ptr, an = sp * (size_t)h->lattice[2];
+    for (const auto& r : h->last_out) {
+        const uintptr_t b = (uintptr_t)r.p;
+        if (r.n && a < b + r.n && b < a + an) return false;
+    }
+    return true;
 }
 
 }  // namespace
@@ -434,6 +479,13 @@ void HPMCbuildHistopyramid(HPMCHistoPyramid* h, GLfloat threshold) {
     V.codes_out = h->codes_capture;
     V.stall_box = h->test_stall_box;
     V.wait_limit_ns = h->test_wait_ns;
+    // alternate the sets: the previous extraction (if still running) reads the other one
+    if (V.column_layout && h->nsets == 2) {
+        h->set ^= 1;
+        V.levels = h->d_levels + (size_t)h->set * h->levels_cap;
+        V.arena = h->d_arena + (size_t)h->set * h->arena_cap * hpmc::kSlotWords;
+    }
+    V.overlap = may_overlap_extraction(h) ? 1 : 0;
     h->threshold = threshold;
     const int max_ctas = h->constants->num_sms * 16;
     cudaError_t e;

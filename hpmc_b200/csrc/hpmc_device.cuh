@@ -83,7 +83,8 @@ struct Ctrl {
     unsigned int work_done;      // traversal CTAs finished (the last one resets the queue)
     unsigned int col_next;       // column classifier's work queue: next column to claim
     unsigned int col_done;       // column classifier CTAs finished (the last one resets the queue)
-    unsigned int pad[4];
+    unsigned int extracting;     // nonzero while an extraction of this pyramid runs (traverse_kernel)
+    unsigned int pad[3];
 };
 
 enum : unsigned int {
@@ -150,7 +151,12 @@ struct Volume {
     // no copy), so the consumers' bounded waits run out and the build reports
     // kStatusTimeout.  -1: off.
     int stall_box;
-    int pad_;
+    // The column classifier may start streaming while the previous grid on
+    // the stream is still this pyramid's extraction (ctrl->extracting set):
+    // the levels and arena it writes are not the ones that extraction reads
+    // (two alternating sets) and the field is none of that extraction's
+    // outputs.  0: every CTA waits for the previous grid first.
+    int overlap;
 };
 
 // --- Morton helpers (X on even bits) ---------------------------------------
@@ -230,7 +236,11 @@ __host__ __device__ __forceinline__ uint64_t column_block_index(const Volume& V,
 // writes global memory that earlier stream work may touch; it returns once
 // the previous grid has completed and its writes are visible (at once when
 // the launch had no such attribute).  allow_next_grid() lets the next kernel
-// launch its CTAs early; they wait in their own wait_prior_grid().
+// launch its CTAs early; they wait in their own wait_prior_grid().  The one
+// exception is the column classifier after its own pyramid's extraction
+// (Volume::overlap): it touches nothing that extraction reads or writes, so
+// its CTAs stream the field at once and wait only before they exit (which
+// keeps the completion order of the stream's grids).
 __device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 

@@ -133,7 +133,7 @@ __device__ __forceinline__ void load_base_tables(TraverseSmem& S) {
 __device__ __forceinline__ void load_tables(const Volume& V, TraverseSmem& S) {
     load_base_tables(S);
     // the pyramid and the control block only after the previous grid (the
-    // build).  No early trigger: the next build launches as these CTAs exit.
+    // build)
     wait_prior_grid();
     for (int i = threadIdx.x; i < V.top_cached; i += blockDim.x) S.top[i] = V.levels[i];
     __syncthreads();
@@ -301,14 +301,16 @@ __device__ __forceinline__ uint32_t next_chunk(const Volume& V, int lane) {
     return __shfl_sync(0xffffffffu, c, 0);
 }
 
-// The last CTA to finish resets the queue for the next launch on the stream.
-__device__ __forceinline__ void finish_queue(const Volume& V) {
+// The last CTA to finish resets the queue for the next launch on the stream
+// (and, after an extraction, clears the pyramid's extraction flag).
+__device__ __forceinline__ void finish_queue(const Volume& V, bool extraction = false) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&V.ctrl->work_done, 1u) == gridDim.x - 1) {
             V.ctrl->work_next = 0;
             V.ctrl->work_done = 0;
+            if (extraction) V.ctrl->extracting = 0;
             __threadfence();
         }
     }
@@ -357,6 +359,17 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
     extern __shared__ __align__(16) uint8_t s_traverse[];
     TraverseSmem& S = *reinterpret_cast<TraverseSmem*>(s_traverse);
     load_tables(V, S);
+    // The next grid (normally the next build) may launch now.  The flag,
+    // written before any CTA of this one lets it launch, tells that build's
+    // column classifier that the previous grid is this extraction, which
+    // neither writes the field nor reads the set of levels and arena that the
+    // build writes next; the last CTA clears it.
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        V.ctrl->extracting = 1u;
+        __threadfence();
+    }
+    __syncthreads();
+    allow_next_grid();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long total = V.ctrl->total;
     const uint32_t N = (uint32_t)(total < O.capacity ? total : O.capacity);
@@ -395,7 +408,7 @@ __global__ void __launch_bounds__(kThreads, 4) traverse_kernel(const __grid_cons
             if (EXTRA && O.dbg_t) O.dbg_t[o] = t;
         }
     }
-    finish_queue(V);
+    finish_queue(V, true);
 }
 
 }  // namespace hpmc

@@ -453,17 +453,26 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
         nlayers = min(V.cells[2], z0 + V.column_slices) - z0 + 1;
     };
 
+    __shared__ int s_early;
     C.cnt[tid] = c_vertex_count[tid];
     fill_slice_table(V, C);
     if (tid == 0) {
         for (int s = 0; s < kRingStages; s++) mbar_init(&C.bar[s], 1);
         mbar_fence_init();
+        // The previous grid may still be this pyramid's extraction (its
+        // flag is set before it lets this launch begin and cleared by its
+        // last CTA): then this CTA streams at once and waits at its end.  A
+        // CTA that sees the flag clear takes the ordinary path; a stale clear
+        // flag only costs the overlap.
+        s_early = V.overlap && *reinterpret_cast<volatile unsigned int*>(&V.ctrl->extracting) != 0u;
     }
-    // global memory (field, pyramid, control block) only after the previous
-    // grid.  No early trigger: the reduce launches as these CTAs exit (reduce
-    // CTAs resident and waiting through the whole build measured ~2% slower).
-    wait_prior_grid();
     __syncthreads();
+    const bool early = s_early != 0;
+    // Otherwise global memory (field, pyramid, control block) only after the
+    // previous grid.  No early trigger: the reduce launches as these CTAs
+    // exit (reduce CTAs resident and waiting through the whole build measured
+    // ~2% slower).
+    if (!early) wait_prior_grid();
     // producer state (thread 0): next box to issue = box pk of column pu; the
     // following column is claimed one column ahead (pnext), so the atomic's
     // round trip overlaps the current column
@@ -543,6 +552,9 @@ __global__ void __launch_bounds__(kThreads) classify_columns(const __grid_consta
             mbar_wait_bounded(&C.bar[p % kRingStages], (p / kRingStages) & 1u, V.wait_limit_ns, nullptr, 0u);
         atomicOr(&V.ctrl->status, kStatusTimeout);
     }
+    // an early CTA ends only after the extraction it overlapped, so the
+    // reduce (and all later work) still follows every earlier grid
+    if (early) wait_prior_grid();
     // the last CTA to finish resets the column queue for the next launch
     if (tid == 0) {
         __threadfence();

@@ -289,6 +289,98 @@ def test_retaint_between_extractions_stays_stream_ordered(hpmc, oracle):
     hp.close()
 
 
+def test_builds_overlapping_extractions_use_alternate_sets(hpmc, oracle):
+    """A build on the column path may start while the previous extraction of
+    the same pyramid still runs (the traversal lets it launch early): builds
+    alternate between two sets of levels and arena, so the running
+    extraction keeps reading its own.  Two different fields back to back,
+    no host sync and no set-up in between, on a non-blocking stream."""
+    import torch
+
+    from hpmc_b200 import datasets
+
+    dev = torch.device("cuda:0")
+    fa, iso = datasets.cayley(256)
+    fb = np.ascontiguousarray(fa[:, ::-1, :] * np.float32(0.8) + np.float32(0.03))
+    ea = oracle_expect(oracle, fa, iso, normals=1)
+    eb = oracle_expect(oracle, fb, iso, normals=1)
+    assert ea["total"] != eb["total"]
+    ta, tb = torch.from_numpy(fa).to(dev), torch.from_numpy(fb).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    hp = hpmc.HistoPyramid(hpmc.default_constants())
+    hp.set_stream(stream)
+    hp.set_normal_mode(1)
+    hp.set_field_device(ta)
+    th = hpmc.TraversalHandle(hp)
+    outs = [[torch.full((e["total"], 4), float("nan"), dtype=torch.float32, device=dev) for _ in range(2)]
+            for e in (ea, eb) for _ in range(3)]
+    torch.cuda.synchronize()
+    for i in range(3):
+        for j, (t, e) in enumerate(((ta, ea), (tb, eb))):
+            hp.set_field_device(t)
+            hp.build(iso)
+            assert hp.classify_path() == 1
+            p, n = outs[3 * j + i]
+            th.extract_to(p, n, e["total"], sync=False)
+    stream.synchronize()
+    for j, e in enumerate((ea, eb)):
+        for i in range(3):
+            got = outs[3 * j + i][0][:, :3].cpu().numpy().astype(np.float64)
+            dp = np.abs(got - e["pos"])
+            assert np.isfinite(got).all() and dp.max() <= 1e-5 / 255 + 1e-6, (j, i, dp.max())
+    th.close()
+    hp.close()
+
+
+def test_build_on_previous_extraction_output_waits_for_it(hpmc, oracle):
+    """A field that is the previous extraction's output buffer: the build must
+    not start before that extraction ends (its field bytes overlap the
+    extraction's outputs, so it takes the ordinary ordered path).  The second
+    volume, of the same lattice (no set-up in between), is the first one's
+    position buffer read as a 256^3 FP32 field (2.0, above the iso-value 0.5,
+    past the vertices)."""
+    import torch
+
+    from hpmc_b200 import datasets
+
+    dev = torch.device("cuda:0")
+    fa, iso = datasets.cayley(256)
+    ta = torch.from_numpy(fa).to(dev)
+    cap = 256 ** 3 // 4  # the position buffer holds exactly one 256^3 FP32 field
+    stream = torch.cuda.Stream(device=dev)
+    hp = hpmc.HistoPyramid(hpmc.default_constants())
+    hp.set_stream(stream)
+    hp.set_normal_mode(1)
+    hp.set_field_device(ta)
+    th = hpmc.TraversalHandle(hp)
+    pa = torch.full((cap, 4), 2.0, dtype=torch.float32, device=dev)
+    na = torch.empty_like(pa)
+    field_b = pa.view(256, 256, 256)
+    # the second volume's field and expected output, from an ordered first pass
+    hp.build(iso)
+    na_ = th.extract_to(pa, na, cap)
+    assert 0 < na_ < cap
+    fb = field_b.cpu().numpy()
+    eb = oracle_expect(oracle, fb, 0.5, normals=1)
+    pb = torch.empty((eb["total"], 4), dtype=torch.float32, device=dev)
+    nb = torch.empty_like(pb)
+    for _ in range(2):
+        with torch.cuda.stream(stream):
+            pa.fill_(2.0)
+        hp.set_field_device(ta)
+        hp.build(iso)
+        th.extract_to(pa, na, cap, sync=False)
+        hp.set_field_device(field_b)  # the extraction above is still writing it
+        hp.build(0.5)
+        assert hp.classify_path() == 1
+        nv = th.extract_to(pb, nb, eb["total"])
+        assert nv == eb["total"], (nv, eb["total"])
+        dp = np.abs(pb[:, :3].cpu().numpy().astype(np.float64) - eb["pos"])
+        assert dp.max() <= 1e-5 / 255 + 1e-6, dp.max()
+    th.close()
+    hp.close()
+
+
 def test_binary_mode_and_feedback_capture(hpmc, oracle):
     """Binary fields (midpoints + table normals) and the N3F_V3F capture."""
     import torch
