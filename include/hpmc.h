@@ -133,7 +133,19 @@ void HPMCdestroyHandle(struct HPMCHistoPyramid* handle);
 
 /* hpmc.h:460-462 / hpiface.cpp:225-290.  Classifies the field at `threshold`
  * and builds the pyramid on the handle's stream (asynchronous).  Errors set
- * the broken flag. */
+ * the broken flag.
+ *
+ * On the TMA column path a build may start while the handle's previous
+ * extraction on the same stream is still writing its vertices.  Builds on
+ * column layouts alternate between two sets of pyramid levels and block
+ * codes (twice the memory), so the running extraction keeps its own.  The
+ * early start never happens when the field's bytes overlap that
+ * extraction's outputs, or when any other work (a kernel, copy or event
+ * wait) comes between the two calls on the stream; the build is then fully
+ * ordered.  A kernel launched by the
+ * caller with programmatic stream serialization between an extraction and a
+ * build must call cudaGridDependencySynchronize() before it writes the field,
+ * which is the rule for such launches in any case. */
 void HPMCbuildHistopyramid(struct HPMCHistoPyramid* h, GLfloat threshold);
 
 /* hpmc.h:468-469 / hpiface.cpp:293-345.  Vertex count of the last build;
