@@ -59,8 +59,8 @@ FALLBACK_HBM_GBS = 6650.0
 # profiles/traverse_kernel_cayley384.txt).  Build traffic grows with the field
 # and traversal traffic with the vertices, so the 512^3 figure is these
 # ratios times the field bytes and the vertex count.
-BUILD_TRAFFIC_PER_FIELD_BYTE = (226531072 + 7344640 + 1064704) / 226492416
-TRAVERSE_TRAFFIC_PER_VERTEX = (29592320 + 13522176) / 2092962
+BUILD_TRAFFIC_PER_FIELD_BYTE = (226531840 + 6623488 + 1064704) / 226492416
+TRAVERSE_TRAFFIC_PER_VERTEX = (29616896 + 15378688) / 2092962
 
 
 NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e nominal (DGX figure), reported beside the measured copy peak
