@@ -89,14 +89,16 @@ struct HPMCHistoPyramid {
     int nsets = 0;
     int set = 0;                   // the set of the last build
     Ctrl* d_ctrl = nullptr;
-    // the last extraction's outputs (byte ranges) and stream: the next build
-    // overlaps it only on the same stream and with a field that is none of them
+    // the last extraction's outputs (byte ranges), stream and set: the next
+    // build overlaps it only on the same stream, into the other set, and with
+    // a field that is none of those outputs
     struct Range {
         const void* p;
         size_t n;
     };
     Range last_out[5] = {};
     cudaStream_t last_out_stream = nullptr;
+    int last_out_set = 0;
     bool have_last_out = false;
     uint8_t* codes_capture = nullptr;
     CUtensorMap tmap;
@@ -283,16 +285,18 @@ int launch_extract(HPMCTraversalHandle* th, float* pos, float* nrm, float* feedb
     h->last_out[3] = {O.dbg_cell, O.dbg_cell ? cap * sizeof(int4) : 0};
     h->last_out[4] = {O.dbg_t, O.dbg_t ? cap * sizeof(float) : 0};
     h->last_out_stream = h->stream;
+    h->last_out_set = h->set;
     h->have_last_out = true;
     return (h->count_valid && h->count_cached > cap) ? HPMC_ERR_CAPACITY : HPMC_OK;
 }
 
 // A build may overlap the previous extraction (Volume::overlap) when it
-// runs the column classifier on the extraction's stream, captures no codes,
-// and its field bytes are none of the extraction's outputs.
+// runs the column classifier on the extraction's stream, writes the set that
+// extraction does not read (h->set is the build's), captures no codes, and
+// its field bytes are none of the extraction's outputs.
 bool may_overlap_extraction(const HPMCHistoPyramid* h) {
     if (!h->V.column_layout || !h->have_tmap || h->nsets < 2 || h->codes_capture || !h->have_last_out ||
-        h->last_out_stream != h->stream || h->fmode != HPMCHistoPyramid::kArray)
+        h->last_out_stream != h->stream || h->last_out_set == h->set || h->fmode != HPMCHistoPyramid::kArray)
         return false;
     const FieldDesc& f = h->field;
     const size_t es = elem_size(f.type);
